@@ -1,0 +1,191 @@
+/*
+ * tfim.h -- C ABI of the TensorFIM-B200 exact maximal-frequent-itemset engine.
+ *
+ * Plain C types only (pointers, sizes, status codes); no torch or CUDA types cross
+ * this boundary except an opaque `void* stream` (a cudaStream_t, or NULL for the
+ * engine's own stream).  Every call returns a status code; none exits the process.
+ * On failure, tfim_last_error() returns a message for the calling thread.
+ *
+ * The reference (hap04210384/TensorFIM) has no plugin or FFI layer: its boundaries are
+ * the engine's command line and two internal C++ counting functions.  Each entry point
+ * below names the reference interface it replaces.
+ *
+ * Threading: a tfim_ctx may be used by one host thread at a time.  Distinct contexts
+ * are independent.
+ */
+#ifndef TFIM_H
+#define TFIM_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define TFIM_API __attribute__((visibility("default")))
+#else
+#define TFIM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define TFIM_OK            0
+#define TFIM_E_INVALID     1   /* bad argument (null pointer, size, threshold outside (0,1]) */
+#define TFIM_E_CUDA        2   /* a CUDA runtime call failed */
+#define TFIM_E_NOMEM       3   /* host or device allocation failed */
+#define TFIM_E_DEPTH       4   /* an item list longer than the counter supports */
+#define TFIM_E_TIMEOUT     5   /* a bounded device-side wait expired */
+#define TFIM_E_STATE       6   /* call order violated (e.g. results before tfim_mine) */
+#define TFIM_E_IO          7   /* results file could not be written */
+
+typedef struct tfim_ctx tfim_ctx;
+
+/* counting paths */
+#define TFIM_COUNTER_AUTO    0   /* chosen per job from its shape */
+#define TFIM_COUNTER_LOP3    1   /* AND + popc on CUDA cores */
+#define TFIM_COUNTER_TENSOR  2   /* b1 AND+POPC tensor-core MMA */
+
+TFIM_API const char* tfim_version(void);
+TFIM_API const char* tfim_last_error(void);
+
+/* Statistics the reference prints in its results header
+ * (code/engine/src/kernel_bitmap.cu:651-679). */
+typedef struct {
+    int64_t trans_num;            /* transactions, empty lines included */
+    int64_t dimension;            /* distinct item ids */
+    int64_t item_id_min;
+    int64_t item_id_max;          /* largest original id */
+    int64_t item_id_max_dense;    /* the header's itemIDmax: dense ids after compaction */
+    int64_t trans_len_min, trans_len_max;
+    double  trans_len_mean;
+    int64_t trans_num_reduced;    /* rows left after dropping infrequent items and empty rows */
+    int64_t trans_len_red_min, trans_len_red_max;
+    double  trans_len_red_mean;
+    int64_t dimension_reduced;    /* ids with freq/transNum > threshold (strict): the root count */
+    double  support_threshold;
+    double  frequency_threshold;  /* trans_num * support_threshold */
+    int32_t min_count;            /* smallest integer support >= frequency_threshold */
+    int32_t n_survivors;          /* dense ids 0..n_survivors-1 are counted */
+    int32_t n_dense;              /* n_survivors, plus one when id 0 is frequent (parked) */
+    int32_t words_per_row;        /* uint32 words per bitmap row in HBM (multiple of 64) */
+} tfim_db_info;
+
+/*
+ * Build the device database from a transaction set given in host memory as CSR
+ * (row r holds items[row_offsets[r] .. row_offsets[r+1])), with the reference's
+ * semantics: F1 occurrence counts, frequencyThreshold = n_rows * support_threshold,
+ * removal of infrequent items and then empty rows, dense ids for survivors in
+ * ascending original-id order, and a vertical bitmap with one 128-byte-aligned row
+ * per dense id.  Ids must be >= 0.
+ *
+ * Replaces readTransSetFile's successors getItemsFrequenc, reduceTransSet, buildBitmap
+ * and uploadBitmapToGPU (code/engine/src/kernel_bitmap.cu:269-298, 692-703, 342-388;
+ * code/engine/src/kernel_bmma.cu:388-444).
+ */
+TFIM_API int tfim_open_db(const int64_t* row_offsets, const int32_t* items, int64_t n_rows,
+                 double support_threshold, int32_t device, tfim_ctx** out);
+
+/*
+ * Open a context over a vertical bitmap supplied directly: n_rows rows of
+ * ceil(n_bits/32) uint32 words each (row-major, bit t of word t/32 = transaction t).
+ * Rows [0, n_counted) are the counted survivors.  Used by the counting interface and
+ * its tests; tfim_mine needs a context from tfim_open_db.
+ */
+TFIM_API int tfim_open_bitmap(const uint32_t* rows, int32_t n_rows, int64_t n_bits, int32_t n_counted,
+                     int32_t device, tfim_ctx** out);
+
+TFIM_API int tfim_db_info_get(const tfim_ctx* ctx, tfim_db_info* out);
+/* dense id -> original id (n_dense entries) */
+TFIM_API int tfim_dense_to_orig(const tfim_ctx* ctx, int32_t* out);
+/* occurrence count per dense id (n_dense entries) */
+TFIM_API int tfim_dense_freq(const tfim_ctx* ctx, int32_t* out);
+
+/*
+ * Counting interface: a wave of b nodes, node i given by its dense item list
+ * item_lists[list_offsets[i] .. list_offsets[i+1]) (at most 64 items; an empty list
+ * is the all-ones prefix).  Writes counts_out[i*n_counted + e] =
+ * popc(AND of the listed rows & row e) for every counted row e, and
+ * nfreq_out[i] = #{e : counts_out[i*n_counted+e] >= min_count}.
+ * Host buffers; the call returns when the results are in them.
+ *
+ * Replaces getResFrequencyCuda(FI, vector<int>*) (code/engine/src/kernel_bitmap.cu:451-536)
+ * and batchCountBMMA(nodes, out) (code/engine/src/kernel_bmma.cu:772-872): the same
+ * per-node vector minus the trailing slot, which is nfreq_out here.
+ */
+TFIM_API int tfim_count_wave(tfim_ctx* ctx, const int32_t* item_lists, const int64_t* list_offsets,
+                    int32_t b, int32_t min_count, int32_t* counts_out, int32_t* nfreq_out);
+
+/* Choose the counter tfim_count_wave uses: TFIM_COUNTER_AUTO (default), _LOP3 or _TENSOR. */
+TFIM_API int tfim_set_counter(tfim_ctx* ctx, int32_t counter);
+
+/*
+ * Same contract with every buffer in device memory, ordered on `stream`
+ * (NULL = the context's stream); returns after the launches are enqueued.
+ * max_len bounds the list lengths (<= 64).
+ */
+TFIM_API int tfim_count_wave_device(tfim_ctx* ctx, const int32_t* d_item_lists, const int64_t* d_list_offsets,
+                           int32_t b, int32_t max_len, int32_t min_count,
+                           int32_t* d_counts_out, int32_t* d_nfreq_out, void* stream);
+
+/* mining engines */
+#define TFIM_ENGINE_PLAIN    0   /* the reference's search, one counted node per launch */
+#define TFIM_ENGINE_BATCHED  1   /* pruned search counted in waves of families */
+
+typedef struct {
+    int32_t engine;        /* TFIM_ENGINE_* */
+    int32_t counter;       /* TFIM_COUNTER_* */
+    int32_t wave_cap;      /* max family rows per wave; 0 = tuned default */
+    int32_t lookahead;     /* 0 off, 1 on (head-union-tail check), 2 learned proposal */
+    int32_t use_graphs;    /* replay wave launches as CUDA graphs when possible */
+    int32_t reserved[11];
+} tfim_mine_opts;
+
+typedef struct {
+    double  mine_seconds;      /* search + counting, bitmap resident (computation_time) */
+    double  device_ms;         /* CUDA-event span of the whole search on the engine's stream */
+    double  kernel_ms;         /* CUDA-event time of the counting launches */
+    int64_t nodes;             /* itemsets counted */
+    int64_t supports;          /* individual supports counted (sum over counted rows) */
+    int64_t bit_ops;           /* supports x transactions (the roofline unit) */
+    int64_t bytes_alg;         /* algorithmic bytes of the counting launches: every operand
+                                  row read once, every count written once */
+    int64_t waves;
+    int64_t launches;          /* kernels launched by the engine */
+    int64_t count_launches;    /* ... of which counting kernels */
+    int64_t lookaheads;        /* head-union-tail checks issued */
+    int64_t lookahead_hits;    /* ... that were frequent and closed a subtree */
+    int64_t pruned_pep;        /* subtrees closed by equal-support pruning */
+    int64_t n_mfi;
+    int64_t reserved[4];
+} tfim_mine_stats;
+
+TFIM_API void tfim_mine_opts_default(tfim_mine_opts* opts);
+
+/*
+ * Mine the maximal frequent itemsets.  The result set equals the reference engine's
+ * output on the same database and threshold: every X that is maximal among frequent
+ * itemsets over the counted items and whose largest dense id is a root, each with its
+ * exact support.  Replaces the search loop of main (code/engine/src/kernel_bitmap.cu:
+ * 841-894) and runWaveEngine (code/engine/src/kernel_bmma.cu:896-910).
+ */
+TFIM_API int tfim_mine(tfim_ctx* ctx, const tfim_mine_opts* opts, tfim_mine_stats* stats);
+
+TFIM_API int64_t tfim_num_mfis(const tfim_ctx* ctx);
+TFIM_API int64_t tfim_mfi_item_total(const tfim_ctx* ctx);
+/* MFIs sorted by descending support; items in ORIGINAL ids, largest first
+ * (the reference's print order). offsets has num_mfis+1 entries. */
+TFIM_API int tfim_get_mfis(const tfim_ctx* ctx, int32_t* items, int64_t* offsets, int32_t* supports);
+
+/*
+ * Write the reference's results file (code/engine/src/kernel_bitmap.cu:651-690):
+ * header keys, "<i>th: <k> { ids }   support: <s>  frequency: <f>" lines, MFIsNumber.
+ */
+TFIM_API int tfim_write_results(const tfim_ctx* ctx, const char* trans_set_file, const char* result_path,
+                       double preprocessing_s, double computation_s);
+
+TFIM_API void tfim_close(tfim_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TFIM_H */

@@ -1,0 +1,119 @@
+"""ctypes binding of libtfim.so (include/tfim.h).
+
+The library is loaded from tensorfim_b200/_lib/; there is no fallback implementation:
+if it is missing or a call fails, a TfimError is raised.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libtfim.so")
+CLI_PATH = os.path.join(HERE, "_lib", "tfim")
+
+TFIM_OK = 0
+TFIM_E_INVALID = 1
+TFIM_E_CUDA = 2
+TFIM_E_NOMEM = 3
+TFIM_E_DEPTH = 4
+TFIM_E_TIMEOUT = 5
+TFIM_E_STATE = 6
+TFIM_E_IO = 7
+
+ENGINE_PLAIN = 0
+ENGINE_BATCHED = 1
+COUNTER_AUTO = 0
+COUNTER_LOP3 = 1
+COUNTER_TENSOR = 2
+
+# every entry point declared in include/tfim.h
+EXPORTS = [
+    "tfim_version", "tfim_last_error", "tfim_open_db", "tfim_open_bitmap", "tfim_db_info_get",
+    "tfim_dense_to_orig", "tfim_dense_freq", "tfim_count_wave", "tfim_set_counter",
+    "tfim_count_wave_device", "tfim_mine_opts_default", "tfim_mine", "tfim_num_mfis",
+    "tfim_mfi_item_total", "tfim_get_mfis", "tfim_write_results", "tfim_close",
+]
+
+
+class TfimError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"tfim error {code}: {msg}")
+        self.code = code
+
+
+class DbInfo(C.Structure):
+    _fields_ = [
+        ("trans_num", C.c_int64), ("dimension", C.c_int64), ("item_id_min", C.c_int64),
+        ("item_id_max", C.c_int64), ("item_id_max_dense", C.c_int64),
+        ("trans_len_min", C.c_int64), ("trans_len_max", C.c_int64), ("trans_len_mean", C.c_double),
+        ("trans_num_reduced", C.c_int64), ("trans_len_red_min", C.c_int64), ("trans_len_red_max", C.c_int64),
+        ("trans_len_red_mean", C.c_double), ("dimension_reduced", C.c_int64),
+        ("support_threshold", C.c_double), ("frequency_threshold", C.c_double),
+        ("min_count", C.c_int32), ("n_survivors", C.c_int32), ("n_dense", C.c_int32), ("words_per_row", C.c_int32),
+    ]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class MineOpts(C.Structure):
+    _fields_ = [("engine", C.c_int32), ("counter", C.c_int32), ("wave_cap", C.c_int32),
+                ("lookahead", C.c_int32), ("use_graphs", C.c_int32), ("reserved", C.c_int32 * 11)]
+
+
+class MineStats(C.Structure):
+    _fields_ = [("mine_seconds", C.c_double), ("device_ms", C.c_double), ("kernel_ms", C.c_double),
+                ("nodes", C.c_int64), ("supports", C.c_int64), ("bit_ops", C.c_int64), ("bytes_alg", C.c_int64),
+                ("waves", C.c_int64), ("launches", C.c_int64), ("count_launches", C.c_int64),
+                ("lookaheads", C.c_int64), ("lookahead_hits", C.c_int64), ("pruned_pep", C.c_int64),
+                ("n_mfi", C.c_int64), ("reserved", C.c_int64 * 4)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load libtfim.so once; raise if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise TfimError(-1, f"{LIB_PATH} is missing: build it with `python -m tensorfim_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    p = C.c_void_p
+    i32, i64 = C.c_int32, C.c_int64
+    P = C.POINTER
+    L.tfim_version.restype = C.c_char_p
+    L.tfim_last_error.restype = C.c_char_p
+    L.tfim_open_db.argtypes = [p, p, i64, C.c_double, i32, P(p)]
+    L.tfim_open_bitmap.argtypes = [p, i32, i64, i32, i32, P(p)]
+    L.tfim_db_info_get.argtypes = [p, P(DbInfo)]
+    L.tfim_dense_to_orig.argtypes = [p, p]
+    L.tfim_dense_freq.argtypes = [p, p]
+    L.tfim_count_wave.argtypes = [p, p, p, i32, i32, p, p]
+    L.tfim_set_counter.argtypes = [p, i32]
+    L.tfim_count_wave_device.argtypes = [p, p, p, i32, i32, i32, p, p, p]
+    L.tfim_mine_opts_default.argtypes = [P(MineOpts)]
+    L.tfim_mine_opts_default.restype = None
+    L.tfim_mine.argtypes = [p, P(MineOpts), P(MineStats)]
+    L.tfim_num_mfis.argtypes = [p]
+    L.tfim_num_mfis.restype = i64
+    L.tfim_mfi_item_total.argtypes = [p]
+    L.tfim_mfi_item_total.restype = i64
+    L.tfim_get_mfis.argtypes = [p, p, p, p]
+    L.tfim_write_results.argtypes = [p, C.c_char_p, C.c_char_p, C.c_double, C.c_double]
+    L.tfim_close.argtypes = [p]
+    L.tfim_close.restype = None
+    for name in EXPORTS:
+        getattr(L, name)   # raises AttributeError if an export is missing
+    _lib = L
+    return L
+
+
+def check(rc: int) -> None:
+    if rc != TFIM_OK:
+        raise TfimError(rc, lib().tfim_last_error().decode(errors="replace"))

@@ -1,0 +1,390 @@
+// extern "C" entry points of libtfim (declared in include/tfim.h).
+#include <unistd.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <fstream>
+#include <numeric>
+#include <string>
+
+#include "tfim_internal.h"
+
+namespace tfim {
+int ingest_csr(tfim_ctx* c, const int64_t* off, const int32_t* items, int64_t n_rows, double thr);
+int ingest_bitmap(tfim_ctx* c, const uint32_t* rows, int32_t n_rows, int64_t n_bits, int32_t n_counted);
+
+namespace {
+
+int make_ctx(int32_t device, tfim_ctx** out) {
+    TFIM_CHECK(out != nullptr, TFIM_E_INVALID, "null output handle");
+    *out = nullptr;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n <= 0) {
+        cudaGetLastError();
+        set_error("no CUDA device available (%s)", e != cudaSuccess ? cudaGetErrorString(e) : "0 devices");
+        return TFIM_E_CUDA;
+    }
+    TFIM_CHECK(device >= 0 && device < n, TFIM_E_INVALID, "device %d out of range (%d devices)", device, n);
+    TFIM_CUDA(cudaSetDevice(device));
+    tfim_ctx* c = new (std::nothrow) tfim_ctx();
+    TFIM_CHECK(c != nullptr, TFIM_E_NOMEM, "context allocation failed");
+    c->device = device;
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
+        set_error("stream/event creation failed: %s", cudaGetErrorString(cudaGetLastError()));
+        tfim_close(c);
+        return TFIM_E_CUDA;
+    }
+    *out = c;
+    return TFIM_OK;
+}
+
+// Per-node masks + one count job over every counted row (the reference counting contract).
+int count_wave_impl(tfim_ctx* c, int32_t b, int32_t min_count, const int32_t* d_items, const MatDesc* d_mats,
+                    int32_t* d_counts, int32_t* d_nfreq, cudaStream_t s) {
+    const int32_t d = c->n_counted;
+    // masks: one pool row per node
+    TFIM_TRY(c->d_masks.reserve((size_t)b * (size_t)c->W * 4));
+    TFIM_TRY(launch_materialize(c->d_bitmap, c->W, c->d_masks.as<uint32_t>(), d_mats, d_items, b, s));
+    if (d == 0) return launch_nfreq(d_counts, b, 0, min_count, d_nfreq, s);
+    // host-built job/tile tables (independent of the list contents)
+    const int32_t counter = c->counter_pref;
+    const bool b1 = counter == TFIM_COUNTER_TENSOR || (counter == TFIM_COUNTER_AUTO && b >= 16 && d >= 16);
+    std::vector<JobDesc> jobs(1);
+    jobs[0].base_slot = -1; jobs[0].base_item = -1;
+    jobs[0].n_rows = b; jobs[0].n_cols = d; jobs[0].row_off = 0; jobs[0].col_off = 0; jobs[0].out_off = 0;
+    std::vector<RowDesc> rows(b);
+    for (int32_t i = 0; i < b; i++) rows[i] = RowDesc{i, -1};
+    std::vector<int32_t> cols(d);
+    std::iota(cols.begin(), cols.end(), 0);
+    std::vector<TileDesc> tiles;
+    const int64_t W = c->W;
+    if (b1) {
+        const int64_t base = (int64_t)((b + kB1Rows - 1) / kB1Rows) * ((d + kB1Cols - 1) / kB1Cols);
+        int64_t ks = std::max<int64_t>(1, (4LL * 148 + base - 1) / base);
+        ks = std::min<int64_t>(ks, W / 64);
+        const int64_t kslice = ((W / 64 + ks - 1) / ks) * 64;
+        for (int64_t w0 = 0; w0 < W; w0 += kslice)
+            for (int32_t r0 = 0; r0 < b; r0 += kB1Rows)
+                for (int32_t c0 = 0; c0 < d; c0 += kB1Cols)
+                    tiles.push_back(TileDesc{0, r0, std::min(kB1Rows, b - r0), c0, std::min(d, c0 + kB1Cols), (int32_t)w0,
+                                             (int32_t)std::min<int64_t>(W, w0 + kslice), 0});
+    } else {
+        const int64_t chunk = std::min<int64_t>(W, kLop3Chunk);
+        for (int32_t r0 = 0; r0 < b; r0 += kLop3Rows)
+            for (int32_t c0 = 0; c0 < d; c0 += 64)
+                for (int64_t w0 = 0; w0 < W; w0 += chunk)
+                    tiles.push_back(TileDesc{0, r0, std::min(kLop3Rows, b - r0), c0, std::min(d, c0 + 64), (int32_t)w0,
+                                             (int32_t)std::min<int64_t>(W, w0 + chunk), 0});
+    }
+    const size_t o_rows = 64, o_cols = o_rows + ((rows.size() * sizeof(RowDesc) + 15) & ~size_t(15));
+    const size_t o_tiles = o_cols + ((cols.size() * 4 + 15) & ~size_t(15));
+    const size_t total = o_tiles + tiles.size() * sizeof(TileDesc);
+    TFIM_TRY(c->h_scratch[0].reserve(total));
+    TFIM_TRY(c->d_scratch[0].reserve(total));
+    unsigned char* hp = c->h_scratch[0].as<unsigned char>();
+    memcpy(hp, jobs.data(), sizeof(JobDesc));
+    memcpy(hp + o_rows, rows.data(), rows.size() * sizeof(RowDesc));
+    memcpy(hp + o_cols, cols.data(), cols.size() * 4);
+    memcpy(hp + o_tiles, tiles.data(), tiles.size() * sizeof(TileDesc));
+    unsigned char* dp = c->d_scratch[0].as<unsigned char>();
+    TFIM_CUDA(cudaMemcpyAsync(dp, hp, total, cudaMemcpyHostToDevice, s));
+    TFIM_CUDA(cudaMemsetAsync(d_counts, 0, (size_t)b * d * 4, s));
+    CountArgs a;
+    a.bitmap = c->d_bitmap; a.W = W; a.masks = c->d_masks.as<uint32_t>();
+    a.jobs = (const JobDesc*)dp; a.rows = (const RowDesc*)(dp + o_rows); a.cols = (const int32_t*)(dp + o_cols);
+    a.tiles = (const TileDesc*)(dp + o_tiles); a.n_tiles = (int32_t)tiles.size(); a.out = d_counts;
+    TFIM_TRY(b1 ? launch_count_b1(a, s) : launch_count_lop3(a, s));
+    TFIM_TRY(launch_nfreq(d_counts, b, d, min_count, d_nfreq, s));
+    // the host staging buffer may be reused by the next call only after this copy ran
+    TFIM_CUDA(cudaStreamSynchronize(s));
+    return TFIM_OK;
+}
+
+__global__ void k_mats_from_offsets(const int64_t* __restrict__ off, int32_t b, MatDesc* __restrict__ mats) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= b) return;
+    MatDesc m;
+    m.dst = i; m.src = -1; m.off = (int32_t)off[i]; m.n = (int32_t)(off[i + 1] - off[i]);
+    mats[i] = m;
+}
+
+std::string cpu_name() {
+    std::ifstream f("/proc/cpuinfo");
+    std::string line;
+    while (std::getline(f, line))
+        if (line.rfind("model name", 0) == 0) {
+            size_t p = line.find(':');
+            if (p != std::string::npos) {
+                std::string s = line.substr(p + 1);
+                size_t b = s.find_first_not_of(" \t");
+                return b == std::string::npos ? s : s.substr(b);
+            }
+        }
+    return "Unknown CPU";
+}
+
+}  // namespace
+}  // namespace tfim
+
+using namespace tfim;
+
+extern "C" {
+
+int tfim_open_db(const int64_t* row_offsets, const int32_t* items, int64_t n_rows, double support_threshold,
+                 int32_t device, tfim_ctx** out) {
+    TFIM_CHECK(out != nullptr, TFIM_E_INVALID, "null output handle");
+    *out = nullptr;
+    TFIM_CHECK(row_offsets != nullptr && n_rows >= 0, TFIM_E_INVALID, "invalid transaction set");
+    TFIM_CHECK(n_rows == 0 || row_offsets[n_rows] == 0 || items != nullptr, TFIM_E_INVALID, "null items");
+    TFIM_CHECK(support_threshold > 0.0 && support_threshold <= 1.0 && std::isfinite(support_threshold), TFIM_E_INVALID,
+               "support threshold %g outside (0, 1]", support_threshold);
+    tfim_ctx* c = nullptr;
+    TFIM_TRY(make_ctx(device, &c));
+    int rc = ingest_csr(c, row_offsets, items, n_rows, support_threshold);
+    if (rc != TFIM_OK) { tfim_close(c); return rc; }
+    *out = c;
+    return TFIM_OK;
+}
+
+int tfim_open_bitmap(const uint32_t* rows, int32_t n_rows, int64_t n_bits, int32_t n_counted, int32_t device,
+                     tfim_ctx** out) {
+    TFIM_CHECK(out != nullptr, TFIM_E_INVALID, "null output handle");
+    *out = nullptr;
+    tfim_ctx* c = nullptr;
+    TFIM_TRY(make_ctx(device, &c));
+    int rc = ingest_bitmap(c, rows, n_rows, n_bits, n_counted);
+    if (rc != TFIM_OK) { tfim_close(c); return rc; }
+    *out = c;
+    return TFIM_OK;
+}
+
+int tfim_db_info_get(const tfim_ctx* c, tfim_db_info* out) {
+    TFIM_CHECK(c && out, TFIM_E_INVALID, "null argument");
+    *out = c->info;
+    return TFIM_OK;
+}
+
+int tfim_dense_to_orig(const tfim_ctx* c, int32_t* out) {
+    TFIM_CHECK(c && out, TFIM_E_INVALID, "null argument");
+    std::copy(c->dense_to_orig.begin(), c->dense_to_orig.end(), out);
+    return TFIM_OK;
+}
+
+int tfim_dense_freq(const tfim_ctx* c, int32_t* out) {
+    TFIM_CHECK(c && out, TFIM_E_INVALID, "null argument");
+    if (c->from_db) std::copy(c->dense_freq.begin(), c->dense_freq.end(), out);
+    else std::copy(c->bit_support.begin(), c->bit_support.end(), out);
+    return TFIM_OK;
+}
+
+int tfim_set_counter(tfim_ctx* c, int32_t counter) {
+    TFIM_CHECK(c, TFIM_E_INVALID, "null context");
+    TFIM_CHECK(counter >= TFIM_COUNTER_AUTO && counter <= TFIM_COUNTER_TENSOR, TFIM_E_INVALID, "unknown counter %d", counter);
+    c->counter_pref = counter;
+    return TFIM_OK;
+}
+
+int tfim_count_wave(tfim_ctx* c, const int32_t* item_lists, const int64_t* list_offsets, int32_t b, int32_t min_count,
+                    int32_t* counts_out, int32_t* nfreq_out) {
+    TFIM_CHECK(c && list_offsets && counts_out && nfreq_out && b >= 0, TFIM_E_INVALID, "tfim_count_wave: invalid arguments");
+    if (b == 0) return TFIM_OK;
+    TFIM_CUDA(cudaSetDevice(c->device));
+    const int32_t n_rows_total = c->info.n_dense;
+    TFIM_CHECK(list_offsets[0] == 0, TFIM_E_INVALID, "list_offsets[0] must be 0");
+    for (int32_t i = 0; i < b; i++) {
+        const int64_t len = list_offsets[i + 1] - list_offsets[i];
+        TFIM_CHECK(len >= 0, TFIM_E_INVALID, "list_offsets must be non-decreasing");
+        TFIM_CHECK(len <= kMaxListLen, TFIM_E_DEPTH, "node %d lists %lld items; at most %d", i, (long long)len, kMaxListLen);
+        for (int64_t q = list_offsets[i]; q < list_offsets[i + 1]; q++)
+            TFIM_CHECK(item_lists[q] >= 0 && item_lists[q] < n_rows_total, TFIM_E_INVALID, "item %d out of range", item_lists[q]);
+    }
+    const int64_t n_items = list_offsets[b];
+    const int32_t d = c->n_counted;
+    cudaStream_t s = c->stream;
+    // device staging: items, mats, counts, nfreq
+    const size_t o_items = 0;
+    const size_t o_mats = (((size_t)std::max<int64_t>(n_items, 1) * 4) + 15) & ~size_t(15);
+    const size_t o_counts = o_mats + (((size_t)b * sizeof(MatDesc) + 15) & ~size_t(15));
+    const size_t o_nfreq = o_counts + (((size_t)b * d * 4 + 15) & ~size_t(15));
+    const size_t total = o_nfreq + (size_t)b * 4;
+    TFIM_TRY(c->d_scratch[1].reserve(total));
+    TFIM_TRY(c->h_scratch[1].reserve(o_counts));
+    unsigned char* hp = c->h_scratch[1].as<unsigned char>();
+    if (n_items) memcpy(hp + o_items, item_lists, (size_t)n_items * 4);
+    MatDesc* hm = (MatDesc*)(hp + o_mats);
+    for (int32_t i = 0; i < b; i++) hm[i] = MatDesc{i, -1, (int32_t)list_offsets[i], (int32_t)(list_offsets[i + 1] - list_offsets[i])};
+    unsigned char* dp = c->d_scratch[1].as<unsigned char>();
+    TFIM_CUDA(cudaMemcpyAsync(dp, hp, o_counts, cudaMemcpyHostToDevice, s));
+    TFIM_TRY(count_wave_impl(c, b, min_count, (const int32_t*)(dp + o_items), (const MatDesc*)(dp + o_mats),
+                             (int32_t*)(dp + o_counts), (int32_t*)(dp + o_nfreq), s));
+    TFIM_CUDA(cudaMemcpyAsync(counts_out, dp + o_counts, (size_t)b * d * 4, cudaMemcpyDeviceToHost, s));
+    TFIM_CUDA(cudaMemcpyAsync(nfreq_out, dp + o_nfreq, (size_t)b * 4, cudaMemcpyDeviceToHost, s));
+    TFIM_CUDA(cudaStreamSynchronize(s));
+    return TFIM_OK;
+}
+
+int tfim_count_wave_device(tfim_ctx* c, const int32_t* d_item_lists, const int64_t* d_list_offsets, int32_t b,
+                           int32_t max_len, int32_t min_count, int32_t* d_counts_out, int32_t* d_nfreq_out, void* stream) {
+    TFIM_CHECK(c && d_list_offsets && d_counts_out && d_nfreq_out && b >= 0, TFIM_E_INVALID,
+               "tfim_count_wave_device: invalid arguments");
+    TFIM_CHECK(max_len >= 0 && max_len <= kMaxListLen, TFIM_E_DEPTH, "max_len %d exceeds %d", max_len, kMaxListLen);
+    if (b == 0) return TFIM_OK;
+    TFIM_CUDA(cudaSetDevice(c->device));
+    cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+    TFIM_TRY(c->d_scratch[2].reserve((size_t)b * sizeof(MatDesc)));
+    k_mats_from_offsets<<<(b + 255) / 256, 256, 0, s>>>(d_list_offsets, b, c->d_scratch[2].as<MatDesc>());
+    TFIM_CUDA(cudaGetLastError());
+    return count_wave_impl(c, b, min_count, d_item_lists, c->d_scratch[2].as<MatDesc>(), d_counts_out, d_nfreq_out, s);
+}
+
+int tfim_mine(tfim_ctx* c, const tfim_mine_opts* opts, tfim_mine_stats* stats) {
+    TFIM_CHECK(c, TFIM_E_INVALID, "null context");
+    TFIM_CHECK(c->from_db, TFIM_E_STATE, "tfim_mine needs a context opened with tfim_open_db");
+    TFIM_CUDA(cudaSetDevice(c->device));
+    tfim_mine_opts o;
+    if (opts) o = *opts;
+    else tfim_mine_opts_default(&o);
+    tfim_mine_stats st;
+    memset(&st, 0, sizeof st);
+    c->mfi_items.clear();
+    c->mfi_support.clear();
+    c->mined = false;
+    cudaEvent_t e_begin = nullptr, e_end = nullptr;
+    TFIM_CUDA(cudaEventCreate(&e_begin));
+    TFIM_CUDA(cudaEventCreate(&e_end));
+    TFIM_CUDA(cudaEventRecord(e_begin, c->stream));
+    const auto t0 = std::chrono::steady_clock::now();
+    int rc;
+    if (o.engine == TFIM_ENGINE_PLAIN) rc = mine_plain(c, &o, &st);
+    else if (o.engine == TFIM_ENGINE_BATCHED) rc = mine_batched(c, &o, &st);
+    else { set_error("unknown engine %d", o.engine); return TFIM_E_INVALID; }
+    cudaEventRecord(e_end, c->stream);
+    cudaEventSynchronize(e_end);
+    const auto t1 = std::chrono::steady_clock::now();
+    float span_ms = 0;
+    cudaEventElapsedTime(&span_ms, e_begin, e_end);
+    cudaEventDestroy(e_begin);
+    cudaEventDestroy(e_end);
+    if (rc != TFIM_OK) return rc;
+    st.device_ms = span_ms;
+    // descending support; ties by descending item lists (deterministic order)
+    std::vector<size_t> idx(c->mfi_items.size());
+    std::iota(idx.begin(), idx.end(), 0);
+    std::sort(idx.begin(), idx.end(), [&](size_t a, size_t b) {
+        if (c->mfi_support[a] != c->mfi_support[b]) return c->mfi_support[a] > c->mfi_support[b];
+        return c->mfi_items[a] > c->mfi_items[b];
+    });
+    std::vector<std::vector<int32_t>> items(idx.size());
+    std::vector<int32_t> sup(idx.size());
+    for (size_t k = 0; k < idx.size(); k++) { items[k] = std::move(c->mfi_items[idx[k]]); sup[k] = c->mfi_support[idx[k]]; }
+    c->mfi_items.swap(items);
+    c->mfi_support.swap(sup);
+    st.mine_seconds = std::chrono::duration<double>(t1 - t0).count();
+    if (st.bit_ops == 0) st.bit_ops = st.supports * c->n_bits;
+    st.n_mfi = (int64_t)c->mfi_items.size();
+    c->mined = true;
+    c->last_stats = st;
+    if (stats) *stats = st;
+    return TFIM_OK;
+}
+
+int64_t tfim_num_mfis(const tfim_ctx* c) { return c && c->mined ? (int64_t)c->mfi_items.size() : -1; }
+
+int64_t tfim_mfi_item_total(const tfim_ctx* c) {
+    if (!c || !c->mined) return -1;
+    int64_t s = 0;
+    for (auto& v : c->mfi_items) s += (int64_t)v.size();
+    return s;
+}
+
+int tfim_get_mfis(const tfim_ctx* c, int32_t* items, int64_t* offsets, int32_t* supports) {
+    TFIM_CHECK(c && items && offsets && supports, TFIM_E_INVALID, "null argument");
+    TFIM_CHECK(c->mined, TFIM_E_STATE, "tfim_get_mfis before tfim_mine");
+    int64_t o = 0;
+    for (size_t k = 0; k < c->mfi_items.size(); k++) {
+        offsets[k] = o;
+        for (int32_t x : c->mfi_items[k]) items[o++] = c->dense_to_orig[x];
+        supports[k] = c->mfi_support[k];
+    }
+    offsets[c->mfi_items.size()] = o;
+    return TFIM_OK;
+}
+
+int tfim_write_results(const tfim_ctx* c, const char* trans_set_file, const char* result_path, double prep_s,
+                       double comp_s) {
+    TFIM_CHECK(c && trans_set_file && result_path, TFIM_E_INVALID, "null argument");
+    TFIM_CHECK(c->mined, TFIM_E_STATE, "tfim_write_results before tfim_mine");
+    FILE* f = fopen(result_path, "w");
+    TFIM_CHECK(f != nullptr, TFIM_E_IO, "cannot open %s for writing", result_path);
+    const tfim_db_info& I = c->info;
+    fprintf(f, "==================================================================\n");
+    cudaDeviceProp p;
+    if (cudaGetDeviceProperties(&p, c->device) == cudaSuccess) {
+        fprintf(f, "GPU %d: %s\n", c->device, p.name);
+        fprintf(f, "     Multi-Processor Count: %d\n", p.multiProcessorCount);
+        fprintf(f, "     Max Threads Per Multi-Processor: %d\n", p.maxThreadsPerMultiProcessor);
+        fprintf(f, "     Warp Size: %d\n", p.warpSize);
+        fprintf(f, "     Max Threads Per Block: %d\n", p.maxThreadsPerBlock);
+        fprintf(f, "     Compute Capability: %d.%d\n", p.major, p.minor);
+        fprintf(f, "     Number of Multi-Processors: %d\n\n", p.multiProcessorCount);
+    }
+    const long lc = sysconf(_SC_NPROCESSORS_ONLN);
+    fprintf(f, "CPU: %s\n", cpu_name().c_str());
+    fprintf(f, "     Number of Logical Cores: %ld\n\n", lc);
+    int rt = 0;
+    cudaRuntimeGetVersion(&rt);
+    fprintf(f, "CUDA Version: %d.%d\n", rt / 1000, (rt % 1000) / 10);
+    fprintf(f, "Engine: %s\n", tfim_version());
+    fprintf(f, "==================================================================\n");
+    fprintf(f, "transSetFile: %s\n", trans_set_file);
+    fprintf(f, "dimension: %lld\n", (long long)I.dimension);
+    fprintf(f, "transNum: %lld\n", (long long)I.trans_num);
+    fprintf(f, "itemIDmin: %lld\n", (long long)I.item_id_min);
+    fprintf(f, "itemIDmax: %lld\n", (long long)I.item_id_max_dense);
+    fprintf(f, "transLengthMin: %lld\n", (long long)I.trans_len_min);
+    fprintf(f, "transLengthMax: %lld\n", (long long)I.trans_len_max);
+    fprintf(f, "transLengthMean: %g\n", I.trans_len_mean);
+    fprintf(f, "\nsupportThreshold: %g\n\n", I.support_threshold);
+    fprintf(f, "dimensionReduced: %lld\n", (long long)I.dimension_reduced);
+    fprintf(f, "transNumReduced: %lld\n", (long long)I.trans_num_reduced);
+    fprintf(f, "transLengthReducedMin: %lld\n", (long long)I.trans_len_red_min);
+    fprintf(f, "transLengthReducedMax: %lld\n", (long long)I.trans_len_red_max);
+    fprintf(f, "transLengthReducedMean: %g\n", I.trans_len_red_mean);
+    fprintf(f, "\nGPUtaskPercentage: 100%%\n");
+    fprintf(f, "==================================================================\n");
+    fprintf(f, "preprocessing_time(s): %g\n", prep_s);
+    fprintf(f, "computation_time(s): %g\n", comp_s);
+    fprintf(f, "total_time(s): %g\n", prep_s + comp_s);
+    fprintf(f, "\nMFIsNumber: %lld\n", (long long)c->mfi_items.size());
+    fprintf(f, "============================List of MFIs:=============================\n");
+    for (size_t k = 0; k < c->mfi_items.size(); k++) {
+        fprintf(f, "%zuth: %zu { ", k + 1, c->mfi_items[k].size());
+        for (int32_t x : c->mfi_items[k]) fprintf(f, "%d ", c->dense_to_orig[x]);
+        fprintf(f, "}   support: %g  frequency: %d\n", (double)c->mfi_support[k] / (double)I.trans_num, c->mfi_support[k]);
+    }
+    fprintf(f, "==================================================================\n");
+    const bool ok = ferror(f) == 0;
+    fclose(f);
+    TFIM_CHECK(ok, TFIM_E_IO, "write to %s failed", result_path);
+    return TFIM_OK;
+}
+
+void tfim_close(tfim_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->d_bitmap) cudaFree(c->d_bitmap);
+    for (auto& b : c->d_scratch) b.release();
+    for (auto& b : c->h_scratch) b.release();
+    c->d_masks.release();
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+}  // extern "C"

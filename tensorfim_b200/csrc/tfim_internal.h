@@ -1,0 +1,172 @@
+// Internal declarations shared by the engine's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "tfim.h"
+
+namespace tfim {
+
+// ------------------------------------------------------------------ errors
+void set_error(const char* fmt, ...);
+const char* get_error();
+
+#define TFIM_CUDA(call)                                                                    \
+    do {                                                                                   \
+        cudaError_t e__ = (call);                                                          \
+        if (e__ != cudaSuccess) {                                                          \
+            ::tfim::set_error("%s:%d %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(e__)); \
+            return TFIM_E_CUDA;                                                            \
+        }                                                                                  \
+    } while (0)
+
+#define TFIM_CHECK(cond, code, ...)                                                        \
+    do {                                                                                   \
+        if (!(cond)) {                                                                     \
+            ::tfim::set_error(__VA_ARGS__);                                                \
+            return (code);                                                                 \
+        }                                                                                  \
+    } while (0)
+
+#define TFIM_TRY(call)                                                                     \
+    do {                                                                                   \
+        int s__ = (call);                                                                  \
+        if (s__ != TFIM_OK) return s__;                                                    \
+    } while (0)
+
+// ------------------------------------------------------------------ layout
+// Bitmap rows are padded to a multiple of 64 uint32 words (2048 bits, 256 bytes), so
+// every row starts 256-byte aligned and any 2048-bit K-chunk is whole.
+constexpr int kRowAlignWords = 64;
+inline int64_t words_for_bits(int64_t bits) {
+    int64_t w = (bits + 31) / 32;
+    return (w + kRowAlignWords - 1) / kRowAlignWords * kRowAlignWords;
+}
+
+constexpr int kMaxListLen = 64;   // longest item list one counted row may AND
+
+// A device buffer that grows on demand and is freed with the context.
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    int reserve(size_t need);
+    void release();
+    template <typename T> T* as() const { return reinterpret_cast<T*>(p); }
+};
+struct HostBuf {   // pinned host staging
+    void* p = nullptr;
+    size_t bytes = 0;
+    int reserve(size_t need);
+    void release();
+    template <typename T> T* as() const { return reinterpret_cast<T*>(p); }
+};
+
+// ------------------------------------------------------------------ count jobs
+// A count job: a base mask along the transaction axis (a mask-pool row AND an item row,
+// either optional), a set of counted rows and a set of columns (item rows):
+//   out[out_off + r*n_cols + c] = popc(base & A_r & B[col c])
+//   A_r = (row.slot >= 0 ? masks[row.slot] : ~0) & (row.item >= 0 ? B[row.item] : ~0)
+// A column id of -1 stands for the all-ones column (so the count is popc(base & A_r)).
+struct JobDesc {
+    int32_t base_slot;    // mask-pool row, or -1
+    int32_t base_item;    // bitmap row, or -1
+    int32_t n_rows;
+    int32_t n_cols;
+    int32_t row_off;      // into the RowDesc table
+    int32_t col_off;      // into the column table
+    int64_t out_off;      // into the counts buffer
+};
+struct RowDesc {
+    int32_t slot;
+    int32_t item;
+};
+// One tile: rows [r0, r0+nr) x columns [c0, c1) of job `job` over words [w0, w1).
+struct TileDesc {
+    int32_t job;
+    int32_t r0, nr;
+    int32_t c0, c1;
+    int32_t w0, w1;
+    int32_t pad;
+};
+// Mask build: masks[dst] = (src >= 0 ? masks[src] : ~0) & AND of items[off .. off+n).
+struct MatDesc {
+    int32_t dst, src, off, n;
+};
+// One entry of a compacted count row: column index and its count.
+struct Entry {
+    int32_t col, count;
+};
+
+constexpr int kLop3Rows = 8;        // rows per CUDA-core tile
+constexpr int kLop3Chunk = 1024;    // max words per CUDA-core tile
+constexpr int kB1Rows = 64;         // rows per tensor-core tile
+constexpr int kB1Cols = 64;         // columns per tensor-core tile
+
+struct CountArgs {
+    const uint32_t* bitmap;
+    int64_t W;
+    const uint32_t* masks;
+    const JobDesc* jobs;
+    const RowDesc* rows;
+    const int32_t* cols;
+    const TileDesc* tiles;
+    int32_t n_tiles;
+    int32_t* out;
+};
+
+int launch_count_lop3(const CountArgs& a, cudaStream_t s);
+int launch_count_b1(const CountArgs& a, cudaStream_t s);
+int launch_materialize(const uint32_t* bitmap, int64_t W, uint32_t* masks, const MatDesc* mats,
+                       const int32_t* items, int32_t n, cudaStream_t s);
+// nfreq[g] = #{c < n_cols : counts[g*n_cols + c] >= min_count} for g < n_rows
+int launch_nfreq(const int32_t* counts, int64_t n_rows, int32_t n_cols, int32_t min_count,
+                 int32_t* nfreq, cudaStream_t s);
+// For each job row g (global row index over all jobs, row_job[g] = its job):
+// entries >= min_count are appended to `entries` (one atomic reservation per row) and
+// row_info[g] = (start, len).  counter[0] ends as the total entry count.
+int launch_compact(const int32_t* counts, const JobDesc* jobs, const int32_t* row_job,
+                   const int32_t* row_local, int64_t n_rows, int32_t min_count, Entry* entries,
+                   int2* row_info, int32_t* counter, cudaStream_t s);
+
+}  // namespace tfim
+
+// ------------------------------------------------------------------ context
+struct tfim_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    tfim_db_info info{};
+    bool from_db = false;
+    // host-side item tables (dense id space)
+    std::vector<int32_t> dense_to_orig;
+    std::vector<int32_t> dense_freq;       // occurrence counts (F1)
+    std::vector<int32_t> items_in_freq_sort;
+    std::vector<int32_t> roots;            // first dimension_reduced of items_in_freq_sort
+    // device bitmap: n_dense rows x W words
+    uint32_t* d_bitmap = nullptr;
+    int64_t W = 0;
+    int64_t n_bits = 0;
+    int32_t n_counted = 0;
+    std::vector<int32_t> bit_support;      // popc of each counted row (bitmap supports)
+    // scratch
+    tfim::DevBuf d_scratch[8];
+    tfim::HostBuf h_scratch[4];
+    tfim::DevBuf d_masks;                   // mask pool (rows of W words)
+    int64_t mask_slots = 0;
+    // results
+    std::vector<std::vector<int32_t>> mfi_items;  // dense ids
+    std::vector<int32_t> mfi_support;
+    bool mined = false;
+    int32_t counter_pref = TFIM_COUNTER_AUTO;   // counter used by tfim_count_wave
+    tfim_mine_stats last_stats{};
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace tfim {
+int mine_plain(tfim_ctx* ctx, const tfim_mine_opts* o, tfim_mine_stats* st);
+int mine_batched(tfim_ctx* ctx, const tfim_mine_opts* o, tfim_mine_stats* st);
+int compute_bit_supports(tfim_ctx* ctx);
+}  // namespace tfim

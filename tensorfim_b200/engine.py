@@ -1,0 +1,190 @@
+"""Python mirror of the engine's C ABI (include/tfim.h).
+
+The reference exposes two boundaries: the engine command line (``<exe> <transaction file>
+<minsup>`` -> ``<file>-<minsup %f>=Results.txt``, code/engine/src/kernel_bitmap.cu:796-910)
+and its counting contract (``getResFrequencyCuda`` :451-536, ``batchCountBMMA``
+code/engine/src/kernel_bmma.cu:772-872).  ``mine_file`` runs the first through the
+``tfim`` binary; ``Database.count_wave`` is the second; ``Database.mine`` is the search.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+import os
+import subprocess
+
+import numpy as np
+
+from . import _lib
+from ._lib import TfimError, check, lib
+
+ENGINES = {"plain": _lib.ENGINE_PLAIN, "batched": _lib.ENGINE_BATCHED}
+COUNTERS = {"auto": _lib.COUNTER_AUTO, "lop3": _lib.COUNTER_LOP3, "tensor": _lib.COUNTER_TENSOR}
+
+
+def _ptr(a: np.ndarray) -> C.c_void_p:
+    return C.c_void_p(a.ctypes.data) if a.size else C.c_void_p(0)
+
+
+def read_fimi(path: str) -> tuple[np.ndarray, np.ndarray]:
+    """Parse a transaction file with the reference's byte-scanner rules
+    (code/engine/src/kernel_bitmap.cu:205-233): every '\\n' ends a row (empty rows
+    included), digit runs are ids, a digit run right after '-' is dropped, every other
+    byte separates, and a final row without '\\n' counts only when it holds an id.
+    Returns CSR (offsets int64, items int32)."""
+    buf = np.fromfile(path, dtype=np.uint8)
+    n = buf.shape[0]
+    if n == 0:
+        return np.zeros(1, np.int64), np.zeros(0, np.int32)
+    dig = (buf >= 48) & (buf <= 57)
+    prev_dig = np.concatenate([[False], dig[:-1]])
+    starts = np.flatnonzero(dig & ~prev_dig)
+    nxt_dig = np.concatenate([dig[1:], [False]])
+    ends = np.flatnonzero(dig & ~nxt_dig) + 1
+    neg = np.zeros(starts.shape, dtype=bool)
+    has_prev = starts > 0
+    neg[has_prev] = buf[starts[has_prev] - 1] == 45
+    lens = ends - starts
+    vals = np.zeros(starts.shape, dtype=np.int64)
+    for k in range(int(lens.max()) if lens.size else 0):
+        m = lens > k
+        vals[m] = vals[m] * 10 + (buf[starts[m] + k].astype(np.int64) - 48)
+    nl = np.flatnonzero(buf == 10)
+    keep = ~neg
+    tok_row = np.searchsorted(nl, starts[keep], side="left")   # number of newlines before the token
+    items = vals[keep].astype(np.int32)   # (int)long, as the reference
+    n_rows = nl.shape[0]
+    if tok_row.size and tok_row[-1] == n_rows:   # tokens after the last newline form a final row
+        n_rows += 1
+    counts = np.bincount(tok_row, minlength=n_rows)
+    offsets = np.zeros(n_rows + 1, dtype=np.int64)
+    offsets[1:] = np.cumsum(counts)
+    return offsets, items
+
+
+@dataclasses.dataclass
+class MineResult:
+    mfis: list            # [(items: tuple of original ids, largest first), support]
+    stats: dict
+
+    def as_dict(self) -> dict:
+        return {frozenset(items): sup for items, sup in self.mfis}
+
+
+class Database:
+    """A transaction database resident on one GPU (a tfim_ctx)."""
+
+    def __init__(self, handle: C.c_void_p):
+        self._h = handle
+        info = _lib.DbInfo()
+        check(lib().tfim_db_info_get(self._h, C.byref(info)))
+        self.info = info.as_dict()
+
+    # -- construction ------------------------------------------------------------------
+    @classmethod
+    def from_csr(cls, offsets: np.ndarray, items: np.ndarray, minsup: float, device: int = 0) -> "Database":
+        offsets = np.ascontiguousarray(offsets, dtype=np.int64)
+        items = np.ascontiguousarray(items, dtype=np.int32)
+        h = C.c_void_p()
+        check(lib().tfim_open_db(_ptr(offsets), _ptr(items), offsets.shape[0] - 1, float(minsup), device, C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_file(cls, path: str, minsup: float, device: int = 0) -> "Database":
+        off, items = read_fimi(path)
+        return cls.from_csr(off, items, minsup, device)
+
+    @classmethod
+    def from_bitmap(cls, rows: np.ndarray, n_bits: int, n_counted: int, device: int = 0) -> "Database":
+        rows = np.ascontiguousarray(rows, dtype=np.uint32)
+        h = C.c_void_p()
+        check(lib().tfim_open_bitmap(_ptr(rows), rows.shape[0], int(n_bits), int(n_counted), device, C.byref(h)))
+        return cls(h)
+
+    # -- tables --------------------------------------------------------------------------
+    def dense_to_orig(self) -> np.ndarray:
+        out = np.zeros(self.info["n_dense"], dtype=np.int32)
+        check(lib().tfim_dense_to_orig(self._h, _ptr(out)))
+        return out
+
+    def dense_freq(self) -> np.ndarray:
+        out = np.zeros(self.info["n_dense"], dtype=np.int32)
+        check(lib().tfim_dense_freq(self._h, _ptr(out)))
+        return out
+
+    # -- counting contract ---------------------------------------------------------------
+    def count_wave(self, lists: list, min_count: int, counter: str = "auto") -> tuple[np.ndarray, np.ndarray]:
+        """Supports of every counted item against each node's prefix (AND of its dense
+        item list): counts[i, e] and nfreq[i] = #{e : counts[i, e] >= min_count}."""
+        b = len(lists)
+        d = self.info["n_survivors"]
+        offs = np.zeros(b + 1, dtype=np.int64)
+        offs[1:] = np.cumsum([len(x) for x in lists])
+        flat = np.array([x for l in lists for x in l], dtype=np.int32)
+        counts = np.zeros((b, d), dtype=np.int32)
+        nfreq = np.zeros(b, dtype=np.int32)
+        check(lib().tfim_set_counter(self._h, COUNTERS[counter]))
+        check(lib().tfim_count_wave(self._h, _ptr(flat), _ptr(offs), b, int(min_count), _ptr(counts), _ptr(nfreq)))
+        return counts, nfreq
+
+    def count_wave_device(self, d_items: int, d_offsets: int, b: int, max_len: int, min_count: int,
+                          d_counts: int, d_nfreq: int, stream: int = 0) -> None:
+        """Device-pointer form (e.g. torch tensors' data_ptr()), ordered on `stream`."""
+        check(lib().tfim_count_wave_device(self._h, C.c_void_p(d_items), C.c_void_p(d_offsets), int(b), int(max_len),
+                                           int(min_count), C.c_void_p(d_counts), C.c_void_p(d_nfreq),
+                                           C.c_void_p(stream or None)))
+
+    # -- search ----------------------------------------------------------------------------
+    def mine(self, engine: str = "batched", counter: str = "auto", lookahead: bool = True,
+             wave_cap: int = 0) -> MineResult:
+        o = _lib.MineOpts()
+        lib().tfim_mine_opts_default(C.byref(o))
+        o.engine = ENGINES[engine]
+        o.counter = COUNTERS[counter]
+        o.lookahead = int(lookahead)
+        o.wave_cap = int(wave_cap)
+        st = _lib.MineStats()
+        check(lib().tfim_mine(self._h, C.byref(o), C.byref(st)))
+        n = lib().tfim_num_mfis(self._h)
+        tot = lib().tfim_mfi_item_total(self._h)
+        items = np.zeros(max(tot, 1), dtype=np.int32)
+        offs = np.zeros(n + 1, dtype=np.int64)
+        sup = np.zeros(max(n, 1), dtype=np.int32)
+        check(lib().tfim_get_mfis(self._h, _ptr(items), _ptr(offs), _ptr(sup)))
+        mfis = [(tuple(int(x) for x in items[offs[k]:offs[k + 1]]), int(sup[k])) for k in range(n)]
+        return MineResult(mfis, st.as_dict())
+
+    def write_results(self, trans_set_file: str, result_path: str, prep_s: float = 0.0, comp_s: float = 0.0) -> None:
+        check(lib().tfim_write_results(self._h, trans_set_file.encode(), result_path.encode(), prep_s, comp_s))
+
+    def close(self) -> None:
+        if self._h:
+            lib().tfim_close(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def result_path(path: str, minsup: float) -> str:
+    """The reference's result-file name: sprintf("%s-%f=Results.txt") (kernel_bitmap.cu:906-907)."""
+    return "%s-%f=Results.txt" % (path, minsup)
+
+
+def mine_file(path: str, minsup: float, engine: str = "batched", counter: str = "auto", lookahead: int = 1,
+              timeout: float | None = None) -> subprocess.CompletedProcess:
+    """Run the `tfim` command-line engine exactly as a driver runs the reference's exe."""
+    if not os.path.exists(_lib.CLI_PATH):
+        raise TfimError(-1, f"{_lib.CLI_PATH} is missing: build it with `python -m tensorfim_b200.build`")
+    cmd = [_lib.CLI_PATH, path, repr(float(minsup)), "--engine", engine, "--counter", counter,
+           "--lookahead", str(int(lookahead))]
+    return subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)

@@ -1,0 +1,240 @@
+"""Seeded synthetic transaction databases of the five benchmark shapes.
+
+The reference measures on FIMI text files (mushrooms, connect, pumsb_x256, T10I4D100K,
+...).  These generators stand in for them with the shapes named by the benchmark
+configurations; every one uses ``numpy.random.Generator(PCG64(seed))`` and emits item
+ids >= 1 in ascending order within each transaction, with no duplicates and no empty
+lines, so the reference's id-0 and empty-line rules are never triggered by them.
+
+A database is returned as CSR: ``offsets`` (int64, n_rows + 1) and ``items`` (int32).
+``write_fimi`` turns it into the reference's text format (one transaction per line,
+space-separated ids, ``\\n``-terminated), which ``readTransSetFile``
+(code/engine/src/kernel_bitmap.cu:205-267) reads.
+"""
+from __future__ import annotations
+
+import dataclasses
+import numpy as np
+
+__all__ = ["Database", "CONFIGS", "generate", "write_fimi", "categorical", "replicate"]
+
+
+@dataclasses.dataclass
+class Database:
+    offsets: np.ndarray   # int64, n_rows + 1
+    items: np.ndarray     # int32, ids >= 1, ascending within a row
+    n_items: int          # id space is 1..n_items
+    name: str = ""
+    minsup: float = 0.0
+
+    @property
+    def n_rows(self) -> int:
+        return int(self.offsets.shape[0] - 1)
+
+
+def _rng(seed: int) -> np.random.Generator:
+    return np.random.Generator(np.random.PCG64(seed))
+
+
+def categorical(n_rows: int, probs: list[np.ndarray], rng: np.random.Generator, name="", minsup=0.0) -> Database:
+    """One value per attribute group, drawn from that group's categorical ``probs[g]``.
+
+    Group g's values get consecutive ids after the previous groups', starting at 1, so a
+    row lists its ids in ascending order and has exactly len(probs) items."""
+    n_groups = len(probs)
+    base = np.zeros(n_groups, dtype=np.int64)
+    acc = 1
+    for g, p in enumerate(probs):
+        base[g] = acc
+        acc += len(p)
+    cols = np.empty((n_rows, n_groups), dtype=np.int32)
+    for g, p in enumerate(probs):
+        cdf = np.cumsum(p)
+        cdf[-1] = 1.0
+        u = rng.random(n_rows)
+        cols[:, g] = (np.searchsorted(cdf, u, side="right") + base[g]).astype(np.int32)
+    offsets = np.arange(0, (n_rows + 1) * n_groups, n_groups, dtype=np.int64)
+    return Database(offsets, cols.reshape(-1), acc - 1, name, minsup)
+
+
+def replicate(db: Database, factor: int) -> Database:
+    """Exact k-fold concatenation of a database, the reference's replica construction
+    (data/make_replica.py:22-31): every support scales by exactly ``factor``."""
+    n = db.n_rows
+    items = np.tile(db.items, factor)
+    per = db.offsets[-1]
+    offsets = (db.offsets[:-1][None, :] + (np.arange(factor, dtype=np.int64) * per)[:, None]).reshape(-1)
+    offsets = np.concatenate([offsets, np.array([per * factor], dtype=np.int64)])
+    assert offsets.shape[0] == n * factor + 1
+    return Database(offsets, items, db.n_items, db.name, db.minsup)
+
+
+def _cfg1(scale: float = 1.0) -> Database:
+    """Dense categorical: 10,000 rows, 23 groups x 5 values, per-group Dirichlet(0.5)."""
+    rng = _rng(0)
+    probs = [rng.dirichlet(np.full(5, 0.5)) for _ in range(23)]
+    return categorical(int(10_000 * scale), probs, rng, "cfg1_dense_cat_10k", 0.10)
+
+
+def _dominant_probs(rng, n_groups, sizes, lo, hi):
+    probs = []
+    for g in range(n_groups):
+        k = int(sizes[g])
+        p = np.full(k, 0.0)
+        dom = rng.uniform(lo, hi)
+        j = int(rng.integers(k))
+        p[:] = (1.0 - dom) / (k - 1)
+        p[j] = dom
+        probs.append(p)
+    return probs
+
+
+def _cfg2(scale: float = 1.0) -> Database:
+    """Dense categorical, high threshold: 70,000 rows, 43 groups x 3 values, dominant
+    value p ~ U(0.65, 0.95), the rest split evenly."""
+    rng = _rng(1)
+    probs = _dominant_probs(rng, 43, np.full(43, 3), 0.65, 0.95)
+    return categorical(int(70_000 * scale), probs, rng, "cfg2_dense_cat_70k", 0.90)
+
+
+def _cfg3_base(rng) -> tuple[list[np.ndarray], int]:
+    # 2-60 values per group, redrawn until the id space is ~2,100 items
+    while True:
+        sizes = rng.integers(2, 61, size=74)
+        if abs(int(sizes.sum()) - 2100) <= 40:
+            break
+    probs = []
+    for k in sizes:
+        w = np.arange(1, int(k) + 1, dtype=np.float64) ** -1.3
+        w /= w.sum()
+        probs.append(w[rng.permutation(int(k))])
+    return probs, 49_000
+
+
+def _cfg3(scale: float = 1.0, replicas: int = 256) -> Database:
+    """Replicated dense DB: 49,000 base rows x 256 exact replicas, 74 groups of 2-60
+    values, Zipf(s=1.3) within each group."""
+    rng = _rng(2)
+    probs, n = _cfg3_base(rng)
+    base = categorical(int(n * scale), probs, rng, "cfg3_replicated_12.5M", 0.85)
+    return replicate(base, replicas) if replicas > 1 else base
+
+
+def _zipf_sampler(rng, n, s):
+    w = np.arange(1, n + 1, dtype=np.float64) ** -s
+    cdf = np.cumsum(w)
+    cdf /= cdf[-1]
+    perm = rng.permutation(n) + 1   # rank -> item id
+
+    def draw(m):
+        return perm[np.searchsorted(cdf, rng.random(m), side="right").clip(max=n - 1)]
+    return draw
+
+
+def _cfg4(scale: float = 1.0) -> Database:
+    """Sparse long tail: 1,000,000 rows over 40,000 items, length Poisson(10)+1; 70% of
+    each row from a pool of 2,000 patterns (length Poisson(6)+2, weights Exp(1), each
+    pattern item dropped with probability 0.5), the rest Zipf(s=1.1) over the items."""
+    rng = _rng(3)
+    n_items, n_pat = 40_000, 2_000
+    n_rows = int(1_000_000 * scale)
+    pat_len = rng.poisson(6, n_pat) + 2
+    pat_off = np.concatenate([[0], np.cumsum(pat_len)]).astype(np.int64)
+    pat_items = np.concatenate([rng.choice(n_items, int(L), replace=False) + 1 for L in pat_len]).astype(np.int32)
+    pat_w = rng.exponential(1.0, n_pat)
+    pat_cdf = np.cumsum(pat_w) / pat_w.sum()
+    zipf = _zipf_sampler(rng, n_items, 1.1)
+
+    lengths = rng.poisson(10, n_rows) + 1
+    quota = np.rint(0.7 * lengths).astype(np.int64)
+    # up to three pattern instances per row, in draw order; each pattern item survives
+    # corruption with probability 0.5; the first `quota` survivors fill the row
+    K = 3
+    pick = np.searchsorted(pat_cdf, rng.random((n_rows, K)), side="right").clip(max=n_pat - 1)
+    inst_len = pat_len[pick].reshape(-1)                        # per (row, k)
+    inst_row = np.repeat(np.arange(n_rows, dtype=np.int64), K)
+    tot = int(inst_len.sum())
+    inst_start = np.concatenate([[0], np.cumsum(inst_len)[:-1]])
+    within = np.arange(tot, dtype=np.int64) - np.repeat(inst_start, inst_len)
+    src_idx = np.repeat(pat_off[pick.reshape(-1)], inst_len) + within
+    p_items = pat_items[src_idx]
+    p_rows = np.repeat(inst_row, inst_len)
+    keep = rng.random(tot) >= 0.5
+    p_items, p_rows = p_items[keep], p_rows[keep]
+    # rank of each kept item within its row
+    row_first = np.searchsorted(p_rows, np.arange(n_rows), side="left")
+    rank = np.arange(p_rows.shape[0], dtype=np.int64) - row_first[p_rows]
+    take = rank < quota[p_rows]
+    p_items, p_rows = p_items[take], p_rows[take]
+    taken = np.bincount(p_rows, minlength=n_rows)
+    rest = np.maximum(lengths - taken, 0)
+    rest[(taken + rest) == 0] = 1
+    z_rows = np.repeat(np.arange(n_rows, dtype=np.int64), rest)
+    z_items = zipf(int(rest.sum())).astype(np.int64)
+    key = np.concatenate([p_rows * 65536 + p_items, z_rows * 65536 + z_items])
+    key = np.unique(key)
+    rows_of = key >> 16
+    offsets = np.zeros(n_rows + 1, dtype=np.int64)
+    offsets[1:] = np.cumsum(np.bincount(rows_of, minlength=n_rows))
+    items = (key & 65535).astype(np.int32)
+    return Database(offsets, items, n_items, "cfg4_sparse_1M_40k", 0.0005)
+
+
+def _cfg5(scale: float = 1.0) -> Database:
+    """Evaluation DB for the learned proposal: 2,000,000 rows x 60 groups (~500 items),
+    dominant value p ~ U(0.55, 0.9)."""
+    rng = _rng(4)
+    sizes = rng.integers(2, 16, size=60)
+    probs = _dominant_probs(rng, 60, sizes, 0.55, 0.90)
+    return categorical(int(2_000_000 * scale), probs, rng, "cfg5_dense_cat_2M", 0.70)
+
+
+def training_db(kind: int, seed: int, rows: int | None = None) -> Database:
+    """Generators of configurations 1-3 at another seed, used to log lookahead outcomes
+    for training the ordering network (seeds 100-119)."""
+    rng = _rng(seed)
+    if kind == 1:
+        probs = [rng.dirichlet(np.full(5, 0.5)) for _ in range(23)]
+        return categorical(rows or 10_000, probs, rng, f"train1_s{seed}", 0.10)
+    if kind == 2:
+        probs = _dominant_probs(rng, 43, np.full(43, 3), 0.65, 0.95)
+        return categorical(rows or 70_000, probs, rng, f"train2_s{seed}", 0.90)
+    probs, n = _cfg3_base(rng)
+    return categorical(rows or n, probs, rng, f"train3_s{seed}", 0.85)
+
+
+CONFIGS = {1: _cfg1, 2: _cfg2, 3: _cfg3, 4: _cfg4, 5: _cfg5}
+
+
+def generate(cfg: int, **kw) -> Database:
+    return CONFIGS[cfg](**kw)
+
+
+def write_fimi(path: str, db: Database, chunk_rows: int = 1 << 20) -> None:
+    """Write the database as FIMI text: ids separated by one space, one row per line."""
+    with open(path, "wb") as f:
+        for r0 in range(0, db.n_rows, chunk_rows):
+            r1 = min(db.n_rows, r0 + chunk_rows)
+            a, b = int(db.offsets[r0]), int(db.offsets[r1])
+            v = db.items[a:b].astype(np.int64)
+            if v.size == 0:
+                f.write(b"\n" * (r1 - r0))
+                continue
+            nd = np.ones(v.shape, dtype=np.int64)
+            t = v.copy()
+            for _ in range(10):
+                t //= 10
+                nd += (t > 0)
+            width = nd + 1
+            pos = np.concatenate([[0], np.cumsum(width)[:-1]])
+            out = np.empty(int(width.sum()), dtype=np.uint8)
+            for j in range(int(nd.max())):
+                m = nd > j
+                p10 = 10 ** (nd[m] - 1 - j)
+                out[pos[m] + j] = (48 + (v[m] // p10) % 10).astype(np.uint8)
+            # separator after each item: space, or newline after a row's last item
+            sep = np.full(v.shape, 32, dtype=np.uint8)
+            last = (db.offsets[r0 + 1:r1 + 1] - a - 1)
+            sep[last] = 10
+            out[pos + nd] = sep
+            f.write(out.tobytes())

@@ -1,0 +1,119 @@
+"""MFI search on the GPU: set-identical output with identical supports.
+
+Every fixture of tests/golden (produced by the reference engine) is mined by the plain
+engine and by the batched engine under each counter and with lookahead on and off.  At
+full benchmark sizes, where the reference takes too long, the batched engine is checked
+against the plain engine and by the reference's own MFI test (every reported set is
+frequent and no single counted item extends it)."""
+import numpy as np
+import pytest
+
+import tensorfim_b200 as tf
+from tensorfim_b200 import synth
+from conftest import golden_input, golden_names, load_golden
+
+pytestmark = pytest.mark.gpu
+
+VARIANTS = [
+    dict(engine="batched", counter="auto", lookahead=True),
+    dict(engine="batched", counter="lop3", lookahead=True),
+    dict(engine="batched", counter="tensor", lookahead=True),
+    dict(engine="batched", counter="auto", lookahead=False),
+    dict(engine="batched", counter="tensor", lookahead=False, wave_cap=37),
+]
+PLAIN_OK = {"cfg1_full", "cfg2_full", "cfg3_base", "cfg3_base_t30", "cfg4_s001", "cfg5_s002", "edge_dups",
+            "edge_format", "edge_identical", "edge_item0", "edge_none", "edge_single", "edge_ties"}
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_batched_matches_reference(tmp_path, name):
+    fx = load_golden(name)
+    path = golden_input(fx, tmp_path)
+    with tf.Database.from_file(path, fx["spec"]["minsup"]) as db:
+        h = fx["header"]
+        assert db.info["trans_num"] == int(h["transNum"])
+        assert db.info["trans_num_reduced"] == int(h["transNumReduced"])
+        assert db.info["dimension_reduced"] == int(h["dimensionReduced"])
+        assert db.info["dimension"] == int(h["dimension"])
+        assert db.info["item_id_max_dense"] == int(h["itemIDmax"])
+        for v in VARIANTS:
+            res = db.mine(**v)
+            got = res.as_dict()
+            assert len(got) == len(res.mfis), "duplicate MFI reported"
+            assert got == fx["expected"], (v, len(got), len(fx["expected"]))
+
+
+@pytest.mark.parametrize("name", sorted(PLAIN_OK))
+def test_plain_matches_reference(tmp_path, name):
+    fx = load_golden(name)
+    path = golden_input(fx, tmp_path)
+    with tf.Database.from_file(path, fx["spec"]["minsup"]) as db:
+        res = db.mine(engine="plain")
+        assert res.as_dict() == fx["expected"]
+
+
+def test_empty_database():
+    off = np.zeros(1, np.int64)
+    with tf.Database.from_csr(off, np.zeros(0, np.int32), 0.5) as db:
+        assert db.info["trans_num"] == 0
+        assert db.mine().mfis == []
+
+
+def _certify(db, mfis, d2o):
+    """The reference's MFI test on every reported set: support as reported and no counted
+    item outside the set keeps it frequent (nfreq == |X|)."""
+    o2d = {int(o): i for i, o in enumerate(d2o)}
+    lists = [[o2d[x] for x in items] for items, _ in mfis]
+    minc = db.info["min_count"]
+    for s in range(0, len(lists), 512):
+        part = lists[s:s + 512]
+        counts, nfreq = db.count_wave(part, minc)
+        for k, l in enumerate(part):
+            items, sup = mfis[s + k]
+            if len(l) > 1:
+                assert counts[k, l[0]] == sup
+            assert nfreq[k] == len(l)
+
+
+@pytest.mark.slow
+def test_cfg5_full_size_batched_equals_plain():
+    db0 = synth.generate(5)
+    with tf.Database.from_csr(db0.offsets, db0.items, 0.70) as db:
+        a = db.mine(engine="batched")
+        b = db.mine(engine="plain")
+        assert a.as_dict() == b.as_dict()
+        _certify(db, a.mfis, db.dense_to_orig())
+
+
+@pytest.mark.slow
+def test_cfg4_scaled_matches_oracle(oracle_mod, tmp_path):
+    db0 = synth.generate(4, scale=0.05)
+    p = str(tmp_path / "c4.txt")
+    synth.write_fimi(p, db0)
+    exp = oracle_mod.mine_file(p, 0.002)
+    with tf.Database.from_csr(db0.offsets, db0.items, 0.002) as db:
+        for counter in ("auto", "lop3", "tensor"):
+            assert db.mine(counter=counter).as_dict() == exp
+
+
+@pytest.mark.slow
+def test_cfg4_full_size_certified():
+    db0 = synth.generate(4)
+    with tf.Database.from_csr(db0.offsets, db0.items, 0.0005) as db:
+        res = db.mine()
+        assert len(res.mfis) > 1000
+        _certify(db, res.mfis, db.dense_to_orig())
+
+
+@pytest.mark.slow
+def test_cfg3_replicated_matches_base_scaled():
+    """Exact replication scales every support by the factor: the replicated DB's MFIs are
+    the base DB's with supports x factor (data/make_replica.py:1-13)."""
+    base = synth.generate(3, replicas=1, scale=0.1)
+    rep = synth.replicate(base, 64)
+    with tf.Database.from_csr(base.offsets, base.items, 0.3) as db:
+        a = db.mine().as_dict()
+    with tf.Database.from_csr(rep.offsets, rep.items, 0.3) as db:
+        b = db.mine().as_dict()
+    assert b == {k: v * 64 for k, v in a.items()}
+    assert len(a) > 10

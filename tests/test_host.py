@@ -1,0 +1,124 @@
+"""Host-side logic that needs no GPU: parser, generators, results files, the C ABI's
+exports and argument checks, and the command-line front end's failure paths."""
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import tensorfim_b200 as tf
+from tensorfim_b200 import _lib, synth
+from conftest import GOLDEN, ROOT, golden_input, load_golden
+
+
+def _declared_symbols():
+    src = open(os.path.join(ROOT, "include", "tfim.h")).read()
+    return sorted(set(re.findall(r"TFIM_API\s+[\w\s\*]+?\b(tfim_\w+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_symbol():
+    import ctypes
+    declared = _declared_symbols()
+    assert len(declared) >= 17
+    assert sorted(declared) == sorted(_lib.EXPORTS)
+    L = ctypes.CDLL(_lib.LIB_PATH)
+    for name in declared:
+        assert hasattr(L, name), name
+    assert b"sm_100a" in _lib.lib().tfim_version()
+
+
+def test_invalid_threshold_is_rejected_before_any_device_work():
+    off = np.array([0, 2], np.int64)
+    items = np.array([1, 2], np.int32)
+    for thr in (0.0, -0.1, 1.5, float("nan")):
+        with pytest.raises(tf.TfimError) as e:
+            tf.Database.from_csr(off, items, thr)
+        assert e.value.code == _lib.TFIM_E_INVALID
+
+
+def _has_gpu():
+    try:
+        r = subprocess.run(["nvidia-smi", "-L"], capture_output=True, text=True, timeout=20)
+        return r.returncode == 0 and "GPU" in r.stdout
+    except Exception:
+        return False
+
+
+@pytest.mark.skipif(_has_gpu(), reason="checks the behaviour on a machine without a GPU")
+def test_no_gpu_fails_loudly():
+    off = np.array([0, 2], np.int64)
+    items = np.array([1, 2], np.int32)
+    with pytest.raises(tf.TfimError) as e:
+        tf.Database.from_csr(off, items, 0.5)
+    assert e.value.code == _lib.TFIM_E_CUDA
+
+
+def test_cli_usage_and_missing_file(tmp_path):
+    assert os.path.exists(_lib.CLI_PATH)
+    r = subprocess.run([_lib.CLI_PATH], capture_output=True, text=True)
+    assert r.returncode == 1
+    r = subprocess.run([_lib.CLI_PATH, str(tmp_path / "nope.txt"), "0.5"], capture_output=True, text=True)
+    assert r.returncode == 1 and "open failed!" in r.stdout
+
+
+@pytest.mark.parametrize("name", ["edge_format", "edge_dups", "edge_item0", "edge_single", "cfg1_full"])
+def test_read_fimi_matches_oracle_parse(oracle_mod, tmp_path, name):
+    """The Python parser (Database.from_file) follows the reference byte scanner: same row
+    count (empty lines included), same reduced rows."""
+    fx = load_golden(name)
+    path = golden_input(fx, tmp_path)
+    off, items = tf.read_fimi(path)
+    assert off.shape[0] - 1 == int(fx["header"]["transNum"])
+    assert int(items.max(initial=0)) <= 10**9
+    lens = np.diff(off)
+    assert lens.min(initial=0) >= 0
+    if fx["header"]["transLengthMax"] is not None and off.shape[0] > 1:
+        assert lens.max() == int(fx["header"]["transLengthMax"])
+
+
+def test_read_fimi_edge_bytes(tmp_path):
+    p = tmp_path / "x.txt"
+    p.write_bytes(b"1 2\r\n\n-3 4 -5\n7x8\t9\n10")
+    off, items = tf.read_fimi(str(p))
+    assert list(np.diff(off)) == [2, 0, 1, 3, 1]
+    assert list(items) == [1, 2, 4, 7, 8, 9, 10]
+    p.write_bytes(b"1 2\n\n")
+    off, items = tf.read_fimi(str(p))
+    assert list(np.diff(off)) == [2, 0]
+
+
+def test_synth_shapes_and_determinism():
+    a = synth.generate(1)
+    b = synth.generate(1)
+    assert a.n_rows == 10_000 and (a.items == b.items).all()
+    assert (np.diff(a.offsets) == 23).all() and a.n_items == 115
+    c = synth.generate(2, scale=0.1)
+    assert c.n_items == 129 and (np.diff(c.offsets) == 43).all()
+    d = synth.generate(3, replicas=2, scale=0.01)
+    assert d.n_rows == 2 * 490 and abs(d.n_items - 2100) <= 40
+    assert (d.items[: d.offsets[490]] == d.items[d.offsets[490]:]).all()
+    e = synth.generate(4, scale=0.002)
+    assert e.n_rows == 2000 and e.items.min() >= 1 and e.items.max() <= 40_000
+    rows_sorted = all((np.diff(e.items[e.offsets[r]:e.offsets[r + 1]]) > 0).all() for r in range(e.n_rows))
+    assert rows_sorted
+    f = synth.generate(5, scale=0.001)
+    assert (np.diff(f.offsets) == 60).all() and 400 <= f.n_items <= 600
+
+
+def test_write_fimi_round_trip(tmp_path):
+    db = synth.generate(4, scale=0.001)
+    p = str(tmp_path / "r.txt")
+    synth.write_fimi(p, db)
+    off, items = tf.read_fimi(p)
+    assert (off == db.offsets).all() and (items == db.items).all()
+
+
+def test_results_parser_and_compare(tmp_path):
+    p = tmp_path / "r.txt"
+    p.write_text("MFIsNumber: 2\n1th: 2 { 9 3 }   support: 0.5  frequency: 50\n2th: 1 { 4 }   support: 0.4  frequency: 40\n")
+    r = tf.load_results(str(p))
+    assert r == {frozenset({3, 9}): 50, frozenset({4}): 40}
+    assert tf.load_header(str(p))["MFIsNumber"] == "2"
+    c = tf.compare(r, {frozenset({3, 9}): 51})
+    assert not c["identical"] and c["freq_mismatch"] == [((3, 9), 50, 51)]
