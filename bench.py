@@ -176,7 +176,7 @@ def main() -> int:
     ap.add_argument("--workload", default="cfg4", choices=sorted(WORKLOADS))
     ap.add_argument("--counter", default="auto", choices=["auto", "lop3", "tensor"])
     ap.add_argument("--lookahead", type=int, default=1)
-    ap.add_argument("--ref-scale", type=float, default=0.05)
+    ap.add_argument("--ref-scale", type=float, default=0.02)
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")

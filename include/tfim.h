@@ -137,7 +137,9 @@ typedef struct {
     int32_t wave_cap;      /* max family rows per wave; 0 = tuned default */
     int32_t lookahead;     /* 0 off, 1 on (head-union-tail check), 2 learned proposal */
     int32_t use_graphs;    /* replay wave launches as CUDA graphs when possible */
-    int32_t reserved[11];
+    int32_t top_counter;   /* family of the empty prefix: 0 by cost model, 1 bitmap Gram,
+                              2 pair co-occurrence over the reduced transaction list */
+    int32_t reserved[10];
 } tfim_mine_opts;
 
 typedef struct {
@@ -156,7 +158,9 @@ typedef struct {
     int64_t lookahead_hits;    /* ... that were frequent and closed a subtree */
     int64_t pruned_pep;        /* subtrees closed by equal-support pruning */
     int64_t n_mfi;
-    int64_t reserved[4];
+    double  host_ms;           /* host time spent building waves and processing results */
+    double  sync_ms;           /* host time blocked on device results */
+    int64_t reserved[2];
 } tfim_mine_stats;
 
 TFIM_API void tfim_mine_opts_default(tfim_mine_opts* opts);

@@ -59,7 +59,8 @@ class DbInfo(C.Structure):
 
 class MineOpts(C.Structure):
     _fields_ = [("engine", C.c_int32), ("counter", C.c_int32), ("wave_cap", C.c_int32),
-                ("lookahead", C.c_int32), ("use_graphs", C.c_int32), ("reserved", C.c_int32 * 11)]
+                ("lookahead", C.c_int32), ("use_graphs", C.c_int32), ("top_counter", C.c_int32),
+                ("reserved", C.c_int32 * 10)]
 
 
 class MineStats(C.Structure):
@@ -67,7 +68,8 @@ class MineStats(C.Structure):
                 ("nodes", C.c_int64), ("supports", C.c_int64), ("bit_ops", C.c_int64), ("bytes_alg", C.c_int64),
                 ("waves", C.c_int64), ("launches", C.c_int64), ("count_launches", C.c_int64),
                 ("lookaheads", C.c_int64), ("lookahead_hits", C.c_int64), ("pruned_pep", C.c_int64),
-                ("n_mfi", C.c_int64), ("reserved", C.c_int64 * 4)]
+                ("n_mfi", C.c_int64), ("host_ms", C.c_double), ("sync_ms", C.c_double),
+                ("reserved", C.c_int64 * 2)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}

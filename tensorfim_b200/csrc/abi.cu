@@ -271,6 +271,7 @@ int tfim_mine(tfim_ctx* c, const tfim_mine_opts* opts, tfim_mine_stats* stats) {
     cudaEventDestroy(e_end);
     if (rc != TFIM_OK) return rc;
     st.device_ms = span_ms;
+    st.host_ms = std::chrono::duration<double, std::milli>(t1 - t0).count() - st.sync_ms;
     // descending support; ties by descending item lists (deterministic order)
     std::vector<size_t> idx(c->mfi_items.size());
     std::iota(idx.begin(), idx.end(), 0);
@@ -377,7 +378,11 @@ void tfim_close(tfim_ctx* c) {
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->engine) tfim::free_engine(c->engine);
+    c->engine = nullptr;
     if (c->d_bitmap) cudaFree(c->d_bitmap);
+    if (c->d_red_off) cudaFree(c->d_red_off);
+    if (c->d_red_items) cudaFree(c->d_red_items);
     for (auto& b : c->d_scratch) b.release();
     for (auto& b : c->h_scratch) b.release();
     c->d_masks.release();

@@ -30,6 +30,7 @@ struct ScanStats {
     unsigned long long len_sum;
     long long red_min, red_max;
     unsigned long long red_sum;
+    unsigned long long red_sq_sum;   // sum of squared reduced lengths: pair-counting work
 };
 
 __global__ void k_item_minmax(const int32_t* __restrict__ items, int64_t nnz, ScanStats* st) {
@@ -90,19 +91,20 @@ __global__ void k_hist(const int32_t* __restrict__ items, int64_t nnz, int32_t* 
 }
 
 // Per row: the reduced length (occurrences of ids that survive the threshold, id 0
-// included when frequent) and whether the row survives.
+// included when frequent); 0 marks a row that reduction removes.
 __global__ void k_reduced_rows(const int64_t* __restrict__ off, const int32_t* __restrict__ items, int64_t n_rows,
-                               const int32_t* __restrict__ map, int32_t* __restrict__ flag, ScanStats* st) {
+                               const int32_t* __restrict__ map, int32_t* __restrict__ red_len, ScanStats* st) {
     long long mn = LLONG_MAX, mx = 0;
-    unsigned long long sum = 0;
+    unsigned long long sum = 0, sq = 0;
     for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n_rows; r += (int64_t)gridDim.x * blockDim.x) {
         int32_t len = 0;
         for (int64_t j = off[r]; j < off[r + 1]; j++) len += (map[items[j]] >= 0);
-        flag[r] = len > 0;
+        red_len[r] = len;
         if (len > 0) {
             mn = min(mn, (long long)len);
             mx = max(mx, (long long)len);
             sum += (unsigned long long)len;
+            sq += (unsigned long long)len * (unsigned long long)len;
         }
     }
     typedef cub::BlockReduce<long long, 256> BR;
@@ -113,39 +115,59 @@ __global__ void k_reduced_rows(const int64_t* __restrict__ off, const int32_t* _
     __syncthreads();
     long long bmx = BR(t1).Reduce(mx, cub::Max());
     unsigned long long bs = BRU(t2).Sum(sum);
+    __syncthreads();
+    unsigned long long bq = BRU(t2).Sum(sq);
     if (threadIdx.x == 0) {
         atomicMin(&st->red_min, bmn);
         atomicMax(&st->red_max, bmx);
         atomicAdd(&st->red_sum, bs);
+        atomicAdd(&st->red_sq_sum, bq);
     }
 }
 
-// One thread per row: set bit (reduced row index) in the row of every surviving item.
-// Rows of one warp are consecutive, so their bits for one item share a 32-bit word;
-// the warp merges equal (item, word) targets before the atomic.
-__global__ void k_scatter_bits(const int64_t* __restrict__ off, const int32_t* __restrict__ items, int64_t n_rows,
-                               const int32_t* __restrict__ map, const int32_t* __restrict__ flag,
-                               const int64_t* __restrict__ red_idx, uint32_t* __restrict__ bm, int64_t W) {
-    for (int64_t r0 = blockIdx.x * (int64_t)blockDim.x; r0 < n_rows; r0 += (int64_t)gridDim.x * blockDim.x) {
-        int64_t r = r0 + threadIdx.x;
-        bool live = r < n_rows && flag[r];
-        int64_t rr = live ? red_idx[r] : 0;
-        int64_t j = live ? off[r] : 0, je = live ? off[r + 1] : 0;
+struct IsPositive {
+    __host__ __device__ int32_t operator()(int32_t v) const { return v > 0; }
+};
+
+// The reduced transaction list in dense ids (reduced row rr = surviving row r).
+__global__ void k_write_reduced(const int64_t* __restrict__ off, const int32_t* __restrict__ items, int64_t n_rows,
+                                const int32_t* __restrict__ map, const int32_t* __restrict__ red_len,
+                                const int64_t* __restrict__ red_idx, const int64_t* __restrict__ item_off,
+                                int64_t* __restrict__ red_off, int32_t* __restrict__ red_items) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n_rows; r += (int64_t)gridDim.x * blockDim.x) {
+        if (red_len[r] == 0) continue;
+        const int64_t rr = red_idx[r];
+        int64_t o = item_off[r];
+        red_off[rr] = o;
+        for (int64_t j = off[r]; j < off[r + 1]; j++) {
+            const int32_t d = map[items[j]];
+            if (d >= 0) red_items[o++] = d;
+        }
+    }
+}
+
+// One thread per reduced row: set the row's bit in the row of each of its items.  Rows
+// of one warp are consecutive, so their bits for one item share a 32-bit word; the warp
+// merges equal (item, word) targets before the atomic.
+__global__ void k_scatter_bits(const int64_t* __restrict__ red_off, const int32_t* __restrict__ red_items, int64_t n_red,
+                               uint32_t* __restrict__ bm, int64_t W) {
+    for (int64_t r0 = blockIdx.x * (int64_t)blockDim.x; r0 < n_red; r0 += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t rr = r0 + threadIdx.x;
+        const bool live = rr < n_red;
+        int64_t j = live ? red_off[rr] : 0, je = live ? red_off[rr + 1] : 0;
         while (__any_sync(0xffffffffu, j < je)) {
             int32_t d = -1;
-            if (j < je) { d = map[items[j]]; j++; }
-            unsigned long long key = d >= 0 ? ((unsigned long long)(uint32_t)d << 32) | (unsigned long long)(rr >> 5) : ~0ull;
-            unsigned peers = __match_any_sync(0xffffffffu, key);
-            uint32_t bit = d >= 0 ? (1u << (rr & 31)) : 0u;
-            // OR-reduce the bits of this lane's peer group
+            if (j < je) { d = red_items[j]; j++; }
+            const unsigned long long key = d >= 0 ? ((unsigned long long)(uint32_t)d << 32) | (unsigned long long)(rr >> 5) : ~0ull;
+            const unsigned peers = __match_any_sync(0xffffffffu, key);
+            const uint32_t bit = d >= 0 ? (1u << (rr & 31)) : 0u;
             uint32_t acc = bit;
             for (int k = 0; k < 32; k++) {
-                uint32_t v = __shfl_sync(0xffffffffu, bit, k);
+                const uint32_t v = __shfl_sync(0xffffffffu, bit, k);
                 if ((peers >> k) & 1u) acc |= v;
             }
-            int leader = __ffs(peers) - 1;
-            if (d >= 0 && (int)(threadIdx.x & 31) == leader)
-                atomicOr(&bm[(int64_t)d * W + (rr >> 5)], acc);
+            const int leader = __ffs(peers) - 1;
+            if (d >= 0 && (int)(threadIdx.x & 31) == leader) atomicOr(&bm[(int64_t)d * W + (rr >> 5)], acc);
         }
     }
 }
@@ -278,31 +300,51 @@ int ingest_csr(tfim_ctx* c, const int64_t* h_off, const int32_t* h_items, int64_
     const int64_t n_roots = std::min<int64_t>(dimred, n_dense);
     c->roots.assign(c->items_in_freq_sort.begin(), c->items_in_freq_sort.begin() + n_roots);
 
-    // reduced rows and their numbering
+    // reduced rows, their numbering, and the reduced transaction list in dense ids
     if ((rc = d_map.reserve((size_t)(id_max + 1) * 4)) || (rc = d_flag.reserve((size_t)std::max<int64_t>(n_rows, 1) * 4)) ||
-        (rc = d_idx.reserve((size_t)std::max<int64_t>(n_rows, 1) * 8)))
+        (rc = d_idx.reserve((size_t)std::max<int64_t>(n_rows, 1) * 16)))
         return done(rc);
     cudaMemcpyAsync(d_map.p, map.data(), (size_t)(id_max + 1) * 4, cudaMemcpyHostToDevice, s);
-    int64_t n_red = 0;
+    int64_t n_red = 0, n_red_items = 0;
+    int64_t* red_idx = d_idx.as<int64_t>();
+    int64_t* item_off = red_idx + std::max<int64_t>(n_rows, 1);
     if (n_rows > 0) {
+        int32_t* red_len = d_flag.as<int32_t>();
         k_reduced_rows<<<grid_for(n_rows), 256, 0, s>>>(d_off.as<int64_t>(), d_items.as<int32_t>(), n_rows,
-                                                         d_map.as<int32_t>(), d_flag.as<int32_t>(), d_stats.as<ScanStats>());
-        size_t tmp_bytes = 0;
-        cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, d_flag.as<int32_t>(), d_idx.as<int64_t>(), n_rows, s);
-        if ((rc = d_tmp.reserve(tmp_bytes))) return done(rc);
-        cub::DeviceScan::ExclusiveSum(d_tmp.p, tmp_bytes, d_flag.as<int32_t>(), d_idx.as<int64_t>(), n_rows, s);
-        int64_t last_idx = 0;
-        int32_t last_flag = 0;
-        cudaMemcpyAsync(&last_idx, d_idx.as<int64_t>() + (n_rows - 1), 8, cudaMemcpyDeviceToHost, s);
-        cudaMemcpyAsync(&last_flag, d_flag.as<int32_t>() + (n_rows - 1), 4, cudaMemcpyDeviceToHost, s);
+                                                         d_map.as<int32_t>(), red_len, d_stats.as<ScanStats>());
+        cub::TransformInputIterator<int32_t, IsPositive, const int32_t*> flags(red_len, IsPositive());
+        size_t tb1 = 0, tb2 = 0;
+        cub::DeviceScan::ExclusiveSum(nullptr, tb1, flags, red_idx, n_rows, s);
+        cub::DeviceScan::ExclusiveSum(nullptr, tb2, red_len, item_off, n_rows, s);
+        if ((rc = d_tmp.reserve(std::max(tb1, tb2)))) return done(rc);
+        cub::DeviceScan::ExclusiveSum(d_tmp.p, tb1, flags, red_idx, n_rows, s);
+        cub::DeviceScan::ExclusiveSum(d_tmp.p, tb2, red_len, item_off, n_rows, s);
+        int64_t last[2] = {0, 0};
+        int32_t last_len = 0;
+        cudaMemcpyAsync(&last[0], red_idx + (n_rows - 1), 8, cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(&last[1], item_off + (n_rows - 1), 8, cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(&last_len, red_len + (n_rows - 1), 4, cudaMemcpyDeviceToHost, s);
         cudaMemcpyAsync(&hs, d_stats.p, sizeof hs, cudaMemcpyDeviceToHost, s);
         if (cudaStreamSynchronize(s) != cudaSuccess) { set_error("row reduction failed: %s", cudaGetErrorString(cudaGetLastError())); return done(TFIM_E_CUDA); }
-        n_red = last_idx + last_flag;
+        n_red = last[0] + (last_len > 0);
+        n_red_items = last[1] + last_len;
     }
     I.trans_num_reduced = n_red;
     I.trans_len_red_min = n_red > 0 ? hs.red_min : INT_MAX;
     I.trans_len_red_max = n_red > 0 ? hs.red_max : 0;
     I.trans_len_red_mean = (double)hs.red_sum / (double)n_red;   // 0/0 -> nan, as the reference
+    c->red_pair_work = (double)hs.red_sq_sum;
+    if (cudaMalloc(&c->d_red_off, (size_t)(n_red + 1) * 8) != cudaSuccess ||
+        cudaMalloc(&c->d_red_items, (size_t)std::max<int64_t>(n_red_items, 1) * 4) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("reduced transaction list allocation failed");
+        return done(TFIM_E_NOMEM);
+    }
+    c->n_red_items = n_red_items;
+    cudaMemcpyAsync(c->d_red_off + n_red, &n_red_items, 8, cudaMemcpyHostToDevice, s);
+    if (n_red > 0)
+        k_write_reduced<<<grid_for(n_rows), 256, 0, s>>>(d_off.as<int64_t>(), d_items.as<int32_t>(), n_rows, d_map.as<int32_t>(),
+                                                          d_flag.as<int32_t>(), red_idx, item_off, c->d_red_off, c->d_red_items);
 
     // the bitmap: n_dense rows x W words, zero padded
     c->n_bits = n_red;
@@ -316,9 +358,8 @@ int ingest_csr(tfim_ctx* c, const int64_t* h_off, const int32_t* h_items, int64_
         return done(TFIM_E_NOMEM);
     }
     cudaMemsetAsync(c->d_bitmap, 0, bm_bytes, s);
-    if (n_rows > 0 && n_red > 0)
-        k_scatter_bits<<<grid_for(n_rows), 256, 0, s>>>(d_off.as<int64_t>(), d_items.as<int32_t>(), n_rows, d_map.as<int32_t>(),
-                                                        d_flag.as<int32_t>(), d_idx.as<int64_t>(), c->d_bitmap, c->W);
+    if (n_red > 0)
+        k_scatter_bits<<<grid_for(n_red), 256, 0, s>>>(c->d_red_off, c->d_red_items, n_red, c->d_bitmap, c->W);
     if (cudaStreamSynchronize(s) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
         set_error("bitmap scatter failed");
         return done(TFIM_E_CUDA);

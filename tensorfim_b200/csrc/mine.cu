@@ -77,16 +77,25 @@ struct SlotPool {
         *out = n++;
         return TFIM_OK;
     }
+    void reset(tfim_ctx* c) {
+        free_list.clear();
+        deferred.clear();
+        n = 0;
+        cap = c->W > 0 ? (int32_t)std::min<size_t>(c->d_masks.bytes / ((size_t)c->W * 4), INT32_MAX) : 0;
+    }
     void release(int32_t s) { if (s >= 0) deferred.push_back(s); }
     void flush() { free_list.insert(free_list.end(), deferred.begin(), deferred.end()); deferred.clear(); }
 };
 
 // Tile builders --------------------------------------------------------------------------
-void tiles_lop3(int32_t job, int32_t nr, int32_t nc, int64_t W, std::vector<TileDesc>& out) {
+// `upper`: the job's rows and columns are the same list; only tiles holding some (i, j>=i)
+// are emitted and the mirror pass fills the rest.
+void tiles_lop3(int32_t job, int32_t nr, int32_t nc, int64_t W, std::vector<TileDesc>& out, bool upper = false) {
     const int64_t chunk = std::min<int64_t>(W, kLop3Chunk);
     for (int32_t r0 = 0; r0 < nr; r0 += kLop3Rows)
         for (int32_t c0 = 0; c0 < nc; c0 += 64)
             for (int64_t w0 = 0; w0 < W; w0 += chunk) {
+                if (upper && std::min(nc, c0 + 64) <= r0) continue;
                 TileDesc t;
                 t.job = job; t.r0 = r0; t.nr = std::min(kLop3Rows, nr - r0);
                 t.c0 = c0; t.c1 = std::min(nc, c0 + 64);
@@ -95,10 +104,12 @@ void tiles_lop3(int32_t job, int32_t nr, int32_t nc, int64_t W, std::vector<Tile
                 out.push_back(t);
             }
 }
-void tiles_b1(int32_t job, int32_t nr, int32_t nc, int64_t W, int64_t kslice, std::vector<TileDesc>& out) {
+void tiles_b1(int32_t job, int32_t nr, int32_t nc, int64_t W, int64_t kslice, std::vector<TileDesc>& out,
+              bool upper = false) {
     for (int64_t w0 = 0; w0 < W; w0 += kslice)
         for (int32_t r0 = 0; r0 < nr; r0 += kB1Rows)
             for (int32_t c0 = 0; c0 < nc; c0 += kB1Cols) {
+                if (upper && std::min(nc, c0 + kB1Cols) <= r0) continue;
                 TileDesc t;
                 t.job = job; t.r0 = r0; t.nr = std::min(kB1Rows, nr - r0);
                 t.c0 = c0; t.c1 = std::min(nc, c0 + kB1Cols);
@@ -119,9 +130,16 @@ struct Wave {
     std::vector<char> use_b1;    // per job
     int64_t out_total = 0;
     int64_t supports = 0;
+    // the family of the empty prefix (rows == columns): counted as a symmetric bitmap Gram
+    // (top_mode 1) or by pair co-occurrence over the reduced transaction list (top_mode 2)
+    int32_t top_job = -1;
+    int32_t top_mode = 0;
+    std::vector<int32_t> top_pos;    // dense id -> position in the family's list, or -1
+    std::vector<int32_t> top_diag;   // the diagonal: bitmap supports in list order
     void clear() {
         jobs.clear(); rows.clear(); cols.clear(); row_job.clear(); row_local.clear();
         mats.clear(); mat_items.clear(); use_b1.clear(); out_total = 0; supports = 0;
+        top_job = -1; top_mode = 0; top_pos.clear(); top_diag.clear();
     }
     int32_t add_job(int32_t base_slot, int32_t base_item, const std::vector<RowDesc>& rs, const std::vector<int32_t>& cs, bool b1) {
         JobDesc j;
@@ -153,8 +171,17 @@ struct WaveRunner {
     int64_t count_launches = 0;
     int64_t bytes_alg = 0;
     double kernel_ms = 0;
+    double sync_ms = 0;
     int32_t counter = TFIM_COUNTER_AUTO;
     int sm_count = 148;
+
+    void reset_counters() {
+        launches = 0;
+        count_launches = 0;
+        bytes_alg = 0;
+        kernel_ms = 0;
+        sync_ms = 0;
+    }
 
     int run(Wave& w, int32_t min_count, bool want_full_counts, std::vector<int32_t>* full_counts) {
         const int64_t W = c->W;
@@ -162,7 +189,7 @@ struct WaveRunner {
         // split-k factor for tensor tiles: enough tiles to cover the SMs a few times
         int64_t base_b1 = 0;
         for (size_t j = 0; j < w.jobs.size(); j++)
-            if (w.use_b1[j])
+            if (w.use_b1[j] && !((int32_t)j == w.top_job && w.top_mode == 2))
                 base_b1 += (int64_t)((w.jobs[j].n_rows + kB1Rows - 1) / kB1Rows) * ((w.jobs[j].n_cols + kB1Cols - 1) / kB1Cols);
         int64_t kslice = W;
         if (base_b1 > 0) {
@@ -174,12 +201,19 @@ struct WaveRunner {
         const int64_t row_bytes = (c->n_bits + 7) / 8;
         for (size_t j = 0; j < w.jobs.size(); j++) {
             const JobDesc& jd = w.jobs[j];
+            if ((int32_t)j == w.top_job && w.top_mode == 2) {
+                // pair counting reads the reduced transaction list and writes the matrix
+                bytes_alg += (c->d_red_off ? (c->n_bits + 1) * 8 + c->n_red_items * 4 : 0) + 4LL * jd.n_rows * jd.n_cols;
+                continue;
+            }
             const int64_t base_rows = (jd.base_slot >= 0) + (jd.base_item >= 0);
             bytes_alg += row_bytes * (jd.n_rows + jd.n_cols + base_rows) + 4LL * jd.n_rows * jd.n_cols;
         }
         for (size_t j = 0; j < w.jobs.size(); j++) {
-            if (w.use_b1[j]) tiles_b1((int32_t)j, w.jobs[j].n_rows, w.jobs[j].n_cols, W, kslice, t_b1);
-            else tiles_lop3((int32_t)j, w.jobs[j].n_rows, w.jobs[j].n_cols, W, t_l3);
+            const bool top = (int32_t)j == w.top_job;
+            if (top && w.top_mode == 2) continue;
+            if (w.use_b1[j]) tiles_b1((int32_t)j, w.jobs[j].n_rows, w.jobs[j].n_cols, W, kslice, t_b1, top);
+            else tiles_lop3((int32_t)j, w.jobs[j].n_rows, w.jobs[j].n_cols, W, t_l3, top);
         }
         Packer pk;
         const size_t o_jobs = pk.add(w.jobs.data(), w.jobs.size() * sizeof(JobDesc));
@@ -191,6 +225,8 @@ struct WaveRunner {
         const size_t o_rl = pk.add(w.row_local.data(), w.row_local.size() * 4);
         const size_t o_mat = pk.add(w.mats.data(), w.mats.size() * sizeof(MatDesc));
         const size_t o_mi = pk.add(w.mat_items.data(), w.mat_items.size() * 4);
+        const size_t o_tpos = pk.add(w.top_pos.data(), w.top_pos.size() * 4);
+        const size_t o_tdiag = pk.add(w.top_diag.data(), w.top_diag.size() * 4);
         const size_t o_ctr = pk.add(nullptr, 16);
         memset(pk.h.data() + o_ctr, 0, 16);
         TFIM_TRY(h_desc.reserve(pk.h.size()));
@@ -217,6 +253,13 @@ struct WaveRunner {
         a.jobs = (const JobDesc*)(db + o_jobs); a.rows = (const RowDesc*)(db + o_rows);
         a.cols = (const int32_t*)(db + o_cols); a.out = d_counts.as<int32_t>();
         TFIM_CUDA(cudaEventRecord(c->ev0, s));
+        if (w.top_job >= 0 && w.top_mode == 2) {
+            const JobDesc& tj = w.jobs[w.top_job];
+            TFIM_TRY(launch_pair_count(c->d_red_off, c->d_red_items, c->n_bits, (const int32_t*)(db + o_tpos), tj.n_rows,
+                                       d_counts.as<int32_t>() + tj.out_off, s));
+            launches++;
+            count_launches++;
+        }
         if (!t_l3.empty()) {
             a.tiles = (const TileDesc*)(db + o_tl3); a.n_tiles = (int32_t)t_l3.size();
             TFIM_TRY(launch_count_lop3(a, s));
@@ -230,10 +273,18 @@ struct WaveRunner {
             count_launches++;
         }
         TFIM_CUDA(cudaEventRecord(c->ev1, s));
+        if (w.top_job >= 0) {
+            const JobDesc& tj = w.jobs[w.top_job];
+            TFIM_TRY(launch_mirror(d_counts.as<int32_t>() + tj.out_off, tj.n_rows,
+                                   w.top_mode == 2 ? (const int32_t*)(db + o_tdiag) : nullptr, s));
+            launches++;
+        }
         if (want_full_counts) {
             full_counts->resize(w.out_total);
             TFIM_CUDA(cudaMemcpyAsync(full_counts->data(), d_counts.p, (size_t)w.out_total * 4, cudaMemcpyDeviceToHost, s));
+            const double ts0 = now_s();
             TFIM_CUDA(cudaStreamSynchronize(s));
+            sync_ms += (now_s() - ts0) * 1e3;
             float ms = 0;
             cudaEventElapsedTime(&ms, c->ev0, c->ev1);
             kernel_ms += ms;
@@ -249,7 +300,9 @@ struct WaveRunner {
         launches++;
         TFIM_TRY(h_rowinfo.reserve((size_t)(n_rows + 2) * sizeof(int2)));
         TFIM_CUDA(cudaMemcpyAsync(h_rowinfo.p, d_rowinfo.p, (size_t)(n_rows + 1) * sizeof(int2), cudaMemcpyDeviceToHost, s));
+        const double ts0 = now_s();
         TFIM_CUDA(cudaStreamSynchronize(s));
+        sync_ms += (now_s() - ts0) * 1e3;
         float ms = 0;
         cudaEventElapsedTime(&ms, c->ev0, c->ev1);
         kernel_ms += ms;
@@ -260,7 +313,9 @@ struct WaveRunner {
         if (total > 0) {
             TFIM_TRY(h_entries.reserve((size_t)total * sizeof(Entry)));
             TFIM_CUDA(cudaMemcpyAsync(h_entries.p, d_entries.p, (size_t)total * sizeof(Entry), cudaMemcpyDeviceToHost, s));
+            const double ts1 = now_s();
             TFIM_CUDA(cudaStreamSynchronize(s));
+            sync_ms += (now_s() - ts1) * 1e3;
             memcpy(entries.data(), h_entries.p, (size_t)total * sizeof(Entry));
         }
         return TFIM_OK;
@@ -285,8 +340,32 @@ struct MfiSink {
     }
 };
 
+}  // namespace
+
+// Buffers that persist across tfim_mine calls on one context.
+struct EngineState {
+    WaveRunner wr;
+    SlotPool pool;
+};
+
+void free_engine(EngineState* e) {
+    if (!e) return;
+    e->wr.release();
+    delete e;
+}
+
+namespace {
+
+EngineState& engine_state(tfim_ctx* c) {
+    if (!c->engine) c->engine = new EngineState();
+    c->engine->wr.c = c;
+    c->engine->wr.reset_counters();
+    c->engine->pool.reset(c);
+    return *c->engine;
+}
+
 // The reference search for the given roots (pushed in the given order onto a LIFO).
-int run_plain(tfim_ctx* c, const std::vector<int32_t>& roots, WaveRunner& wr, tfim_mine_stats* st) {
+int run_plain(tfim_ctx* c, const std::vector<int32_t>& roots, WaveRunner& wr, SlotPool& pool, tfim_mine_stats* st) {
     struct Node { std::vector<int32_t> items; int32_t freq; int32_t progress; };
     const int32_t d = c->n_counted;
     const int32_t minc = c->info.min_count;
@@ -295,7 +374,6 @@ int run_plain(tfim_ctx* c, const std::vector<int32_t>& roots, WaveRunner& wr, tf
     std::vector<int32_t> counts;
     std::vector<int32_t> all_cols(d);
     std::iota(all_cols.begin(), all_cols.end(), 0);
-    SlotPool pool;
     TFIM_TRY(pool.grow(c, 1));
     Wave w;
     while (!stack.empty()) {
@@ -338,15 +416,15 @@ int run_plain(tfim_ctx* c, const std::vector<int32_t>& roots, WaveRunner& wr, tf
 }  // namespace
 
 int mine_plain(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* st) {
-    WaveRunner wr;
-    wr.c = c;
+    EngineState& es = engine_state(c);
+    WaveRunner& wr = es.wr;
     wr.counter = TFIM_COUNTER_LOP3;
-    int rc = run_plain(c, c->roots, wr, st);
+    int rc = run_plain(c, c->roots, wr, es.pool, st);
     st->launches += wr.launches;
     st->count_launches += wr.count_launches;
     st->bytes_alg += wr.bytes_alg;
     st->kernel_ms += wr.kernel_ms;
-    wr.release();
+    st->sync_ms += wr.sync_ms;
     return rc;
 }
 
@@ -354,8 +432,9 @@ int mine_batched(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* st) {
     const int32_t d = c->n_counted;
     const int32_t minc = c->info.min_count;
     const int64_t W = c->W;
-    WaveRunner wr;
-    wr.c = c;
+    EngineState& es = engine_state(c);
+    WaveRunner& wr = es.wr;
+    SlotPool& pool = es.pool;
     wr.counter = o->counter;
     {
         int dev = 0, n = 0;
@@ -373,15 +452,9 @@ int mine_batched(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* st) {
     if (c->info.n_dense > d) {
         const int32_t parked = d;
         if (sink.is_root[parked]) {
-            WaveRunner pr;
-            pr.c = c;
-            rc = run_plain(c, {parked}, pr, st);
-            st->launches += pr.launches;
-            st->count_launches += pr.count_launches;
-            st->bytes_alg += pr.bytes_alg;
-            st->kernel_ms += pr.kernel_ms;
-            pr.release();
+            rc = run_plain(c, {parked}, wr, pool, st);
             if (rc) return rc;
+            pool.reset(c);
         }
     }
 
@@ -405,7 +478,6 @@ int mine_batched(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* st) {
     std::deque<Fam> fams;   // stable references while children are appended
     std::vector<int32_t> stack;             // family ids, top = back
     std::vector<Look> looks_pending;        // issued with the next wave
-    SlotPool pool;
     const int32_t wave_cap = o->wave_cap > 0 ? o->wave_cap : 4096;
     const bool lookahead = o->lookahead != 0;
 
@@ -419,6 +491,21 @@ int mine_batched(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* st) {
         if (!f.T.empty()) {
             fams.push_back(std::move(f));
             stack.push_back(0);
+        }
+    }
+    // how the family of the empty prefix is counted (whole, in the first wave)
+    int32_t top_mode = 0;
+    if (!fams.empty()) {
+        const double nF = (double)fams[0].F.size();
+        const bool fits = nF * nF * 4.0 <= (double)(1LL << 32);
+        const bool b1 = wr.counter != TFIM_COUNTER_LOP3 && (wr.counter == TFIM_COUNTER_TENSOR || nF >= 16);
+        const double bit_rate = b1 ? kTuneB1BitOps : kTuneLop3BitOps;
+        const double bitmap_s = nF * nF * (double)c->n_bits / 2.0 / bit_rate;
+        const double pairs_s = c->red_pair_work / 2.0 / kTunePairIncrements + nF * nF * 4.0 / kTuneHbmBytes;
+        if (fits) {
+            if (o->top_counter == 1) top_mode = 1;
+            else if (o->top_counter == 2) top_mode = c->d_red_off ? 2 : 1;
+            else top_mode = (c->d_red_off && pairs_s < bitmap_s) ? 2 : 1;
         }
     }
     auto use_b1_for = [&](int32_t nr, int32_t nc) {
@@ -458,10 +545,21 @@ int mine_batched(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* st) {
             if (f.waiting || f.dead) continue;
             const int32_t nT = (int32_t)f.T.size();
             if (f.next_row >= nT) continue;
-            const int32_t take = (int32_t)std::min<int64_t>(nT - f.next_row, wave_cap - rows_taken);
+            const bool whole_top = stack[si] == 0 && top_mode != 0 && f.next_row == 0;
+            const int32_t take = whole_top ? nT : (int32_t)std::min<int64_t>(nT - f.next_row, wave_cap - rows_taken);
             std::vector<RowDesc> rs(take);
             for (int32_t r = 0; r < take; r++) rs[r] = RowDesc{-1, f.T[f.next_row + r]};
             const int32_t job = w.add_job(f.slot, f.item, rs, f.F, use_b1_for(take, (int32_t)f.F.size()));
+            if (whole_top) {
+                w.top_job = job;
+                w.top_mode = top_mode;
+                w.top_pos.assign((size_t)std::max<int32_t>(c->info.n_dense, 1), -1);
+                w.top_diag.resize(f.F.size());
+                for (size_t q = 0; q < f.F.size(); q++) {
+                    w.top_pos[f.F[q]] = (int32_t)q;
+                    w.top_diag[q] = c->bit_support[f.F[q]];
+                }
+            }
             pieces.push_back({stack[si], f.next_row, f.next_row + take, job});
             f.next_row += take;
             rows_taken += take;
@@ -625,9 +723,9 @@ int mine_batched(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* st) {
     st->count_launches += wr.count_launches;
     st->bytes_alg += wr.bytes_alg;
     st->kernel_ms += wr.kernel_ms;
+    st->sync_ms += wr.sync_ms;
     st->bit_ops = st->supports * c->n_bits;
     (void)W;
-    wr.release();
     return TFIM_OK;
 }
 

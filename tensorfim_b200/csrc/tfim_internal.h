@@ -101,6 +101,13 @@ struct Entry {
     int32_t col, count;
 };
 
+// Throughput figures of the counting paths on B200 (measured; used by the engine's cost
+// model to choose how the family of the empty prefix is counted).
+constexpr double kTuneB1BitOps = 1.9e14;       // b1 tensor-core tiles, bit-ops/s
+constexpr double kTuneLop3BitOps = 1.0e14;     // AND+popc tiles, bit-ops/s
+constexpr double kTunePairIncrements = 2.0e10; // pair co-occurrence increments/s
+constexpr double kTuneHbmBytes = 6.5e12;       // bytes/s
+
 constexpr int kLop3Rows = 8;        // rows per CUDA-core tile
 constexpr int kLop3Chunk = 1024;    // max words per CUDA-core tile
 constexpr int kB1Rows = 64;         // rows per tensor-core tile
@@ -120,6 +127,9 @@ struct CountArgs {
 
 int launch_count_lop3(const CountArgs& a, cudaStream_t s);
 int launch_count_b1(const CountArgs& a, cudaStream_t s);
+int launch_pair_count(const int64_t* red_off, const int32_t* red_items, int64_t n_red, const int32_t* pos,
+                      int32_t nF, int32_t* M, cudaStream_t s);
+int launch_mirror(int32_t* M, int32_t nF, const int32_t* diag, cudaStream_t s);
 int launch_materialize(const uint32_t* bitmap, int64_t W, uint32_t* masks, const MatDesc* mats,
                        const int32_t* items, int32_t n, cudaStream_t s);
 // nfreq[g] = #{c < n_cols : counts[g*n_cols + c] >= min_count} for g < n_rows
@@ -133,6 +143,8 @@ int launch_compact(const int32_t* counts, const JobDesc* jobs, const int32_t* ro
                    int2* row_info, int32_t* counter, cudaStream_t s);
 
 }  // namespace tfim
+
+namespace tfim { struct EngineState; }
 
 // ------------------------------------------------------------------ context
 struct tfim_ctx {
@@ -151,6 +163,11 @@ struct tfim_ctx {
     int64_t n_bits = 0;
     int32_t n_counted = 0;
     std::vector<int32_t> bit_support;      // popc of each counted row (bitmap supports)
+    // reduced transaction list (dense ids): row rr = red_items[red_off[rr] .. red_off[rr+1])
+    int64_t* d_red_off = nullptr;
+    int32_t* d_red_items = nullptr;
+    int64_t n_red_items = 0;
+    double red_pair_work = 0;              // sum over reduced rows of length^2
     // scratch
     tfim::DevBuf d_scratch[8];
     tfim::HostBuf h_scratch[4];
@@ -163,9 +180,12 @@ struct tfim_ctx {
     int32_t counter_pref = TFIM_COUNTER_AUTO;   // counter used by tfim_count_wave
     tfim_mine_stats last_stats{};
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    tfim::EngineState* engine = nullptr;
 };
 
 namespace tfim {
+struct EngineState;                        // persistent buffers of the search drivers (mine.cu)
+void free_engine(EngineState* e);
 int mine_plain(tfim_ctx* ctx, const tfim_mine_opts* o, tfim_mine_stats* st);
 int mine_batched(tfim_ctx* ctx, const tfim_mine_opts* o, tfim_mine_stats* st);
 int compute_bit_supports(tfim_ctx* ctx);

@@ -136,13 +136,14 @@ class Database:
 
     # -- search ----------------------------------------------------------------------------
     def mine(self, engine: str = "batched", counter: str = "auto", lookahead: bool = True,
-             wave_cap: int = 0) -> MineResult:
+             wave_cap: int = 0, top: str = "auto") -> MineResult:
         o = _lib.MineOpts()
         lib().tfim_mine_opts_default(C.byref(o))
         o.engine = ENGINES[engine]
         o.counter = COUNTERS[counter]
         o.lookahead = int(lookahead)
         o.wave_cap = int(wave_cap)
+        o.top_counter = {"auto": 0, "bitmap": 1, "pairs": 2}[top]
         st = _lib.MineStats()
         check(lib().tfim_mine(self._h, C.byref(o), C.byref(st)))
         n = lib().tfim_num_mfis(self._h)

@@ -20,6 +20,9 @@ VARIANTS = [
     dict(engine="batched", counter="tensor", lookahead=True),
     dict(engine="batched", counter="auto", lookahead=False),
     dict(engine="batched", counter="tensor", lookahead=False, wave_cap=37),
+    dict(engine="batched", counter="auto", lookahead=True, top="pairs"),
+    dict(engine="batched", counter="lop3", lookahead=False, top="bitmap"),
+    dict(engine="batched", counter="tensor", lookahead=True, top="bitmap"),
 ]
 PLAIN_OK = {"cfg1_full", "cfg2_full", "cfg3_base", "cfg3_base_t30", "cfg4_s001", "cfg5_s002", "edge_dups",
             "edge_format", "edge_identical", "edge_item0", "edge_none", "edge_single", "edge_ties"}
