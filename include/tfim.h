@@ -120,8 +120,8 @@ TFIM_API int tfim_set_counter(tfim_ctx* ctx, int32_t counter);
 
 /*
  * Same contract with every buffer in device memory, ordered on `stream`
- * (NULL = the context's stream); returns after the launches are enqueued.
- * max_len bounds the list lengths (<= 64).
+ * (NULL = the context's stream); returns when the counts are in d_counts_out and
+ * d_nfreq_out.  max_len bounds the list lengths (<= 64).
  */
 TFIM_API int tfim_count_wave_device(tfim_ctx* ctx, const int32_t* d_item_lists, const int64_t* d_list_offsets,
                            int32_t b, int32_t max_len, int32_t min_count,
@@ -160,7 +160,8 @@ typedef struct {
     int64_t n_mfi;
     double  host_ms;           /* host time spent building waves and processing results */
     double  sync_ms;           /* host time blocked on device results */
-    int64_t reserved[2];
+    int64_t lookaheads_skipped;/* lookaheads ruled out because a tail pair is infrequent */
+    int64_t reserved[1];
 } tfim_mine_stats;
 
 TFIM_API void tfim_mine_opts_default(tfim_mine_opts* opts);

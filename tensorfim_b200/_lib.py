@@ -69,7 +69,7 @@ class MineStats(C.Structure):
                 ("waves", C.c_int64), ("launches", C.c_int64), ("count_launches", C.c_int64),
                 ("lookaheads", C.c_int64), ("lookahead_hits", C.c_int64), ("pruned_pep", C.c_int64),
                 ("n_mfi", C.c_int64), ("host_ms", C.c_double), ("sync_ms", C.c_double),
-                ("reserved", C.c_int64 * 2)]
+                ("lookaheads_skipped", C.c_int64), ("reserved", C.c_int64 * 1)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}

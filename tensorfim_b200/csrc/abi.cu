@@ -38,6 +38,8 @@ int make_ctx(int32_t device, tfim_ctx** out) {
         tfim_close(c);
         return TFIM_E_CUDA;
     }
+    for (auto& b : c->d_scratch) b.stream = c->stream;
+    c->d_masks.stream = c->stream;
     *out = c;
     return TFIM_OK;
 }
@@ -91,6 +93,11 @@ int count_wave_impl(tfim_ctx* c, int32_t b, int32_t min_count, const int32_t* d_
     memcpy(hp + o_cols, cols.data(), cols.size() * 4);
     memcpy(hp + o_tiles, tiles.data(), tiles.size() * sizeof(TileDesc));
     unsigned char* dp = c->d_scratch[0].as<unsigned char>();
+    if (s != c->stream) {
+        // buffers are allocated in the context stream's order: the caller's stream waits
+        TFIM_CUDA(cudaEventRecord(c->ev0, c->stream));
+        TFIM_CUDA(cudaStreamWaitEvent(s, c->ev0, 0));
+    }
     TFIM_CUDA(cudaMemcpyAsync(dp, hp, total, cudaMemcpyHostToDevice, s));
     TFIM_CUDA(cudaMemsetAsync(d_counts, 0, (size_t)b * d * 4, s));
     CountArgs a;
@@ -236,6 +243,11 @@ int tfim_count_wave_device(tfim_ctx* c, const int32_t* d_item_lists, const int64
     TFIM_CUDA(cudaSetDevice(c->device));
     cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
     TFIM_TRY(c->d_scratch[2].reserve((size_t)b * sizeof(MatDesc)));
+    TFIM_TRY(c->d_masks.reserve((size_t)b * (size_t)c->W * 4));
+    if (s != c->stream) {
+        TFIM_CUDA(cudaEventRecord(c->ev0, c->stream));
+        TFIM_CUDA(cudaStreamWaitEvent(s, c->ev0, 0));
+    }
     k_mats_from_offsets<<<(b + 255) / 256, 256, 0, s>>>(d_list_offsets, b, c->d_scratch[2].as<MatDesc>());
     TFIM_CUDA(cudaGetLastError());
     return count_wave_impl(c, b, min_count, d_item_lists, c->d_scratch[2].as<MatDesc>(), d_counts_out, d_nfreq_out, s);
@@ -380,12 +392,13 @@ void tfim_close(tfim_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->engine) tfim::free_engine(c->engine);
     c->engine = nullptr;
-    if (c->d_bitmap) cudaFree(c->d_bitmap);
-    if (c->d_red_off) cudaFree(c->d_red_off);
-    if (c->d_red_items) cudaFree(c->d_red_items);
+    tfim::dev_free(c->d_bitmap, c->stream);
+    tfim::dev_free(c->d_red_off, c->stream);
+    tfim::dev_free(c->d_red_items, c->stream);
     for (auto& b : c->d_scratch) b.release();
     for (auto& b : c->h_scratch) b.release();
     c->d_masks.release();
+    if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->stream) cudaStreamDestroy(c->stream);

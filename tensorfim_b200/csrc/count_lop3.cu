@@ -15,51 +15,61 @@ namespace {
 __device__ __forceinline__ uint4 and4(uint4 a, uint4 b) { return make_uint4(a.x & b.x, a.y & b.y, a.z & b.z, a.w & b.w); }
 __device__ __forceinline__ uint32_t popc4(uint4 a) { return __popc(a.x) + __popc(a.y) + __popc(a.z) + __popc(a.w); }
 
-// Block: 256 threads.  Shared memory: kLop3Rows x (w1-w0) words.
+// Block: 256 threads.  Shared memory: kLop3Rows x kLop3Chunk words.  A tile may span
+// any word range; it is processed kLop3Chunk words at a time.
 __global__ void __launch_bounds__(256) k_count_lop3(CountArgs a) {
     extern __shared__ uint4 sm4[];
+    __shared__ const uint4* rsrc[kLop3Rows][2];
     const TileDesc t = a.tiles[blockIdx.x];
     const JobDesc j = a.jobs[t.job];
-    const int nw4 = (t.w1 - t.w0) >> 2;
     const int64_t W = a.W;
-    const uint4* base_m = j.base_slot >= 0 ? reinterpret_cast<const uint4*>(a.masks + (int64_t)j.base_slot * W + t.w0) : nullptr;
-    const uint4* base_i = j.base_item >= 0 ? reinterpret_cast<const uint4*>(a.bitmap + (int64_t)j.base_item * W + t.w0) : nullptr;
-    // 1. stage the tile's row masks for this word chunk
-    for (int r = 0; r < t.nr; r++) {
-        const RowDesc rd = a.rows[j.row_off + t.r0 + r];
-        const uint4* rs = rd.slot >= 0 ? reinterpret_cast<const uint4*>(a.masks + (int64_t)rd.slot * W + t.w0) : nullptr;
-        const uint4* ri = rd.item >= 0 ? reinterpret_cast<const uint4*>(a.bitmap + (int64_t)rd.item * W + t.w0) : nullptr;
-        for (int w = threadIdx.x; w < nw4; w += blockDim.x) {
-            uint4 m = make_uint4(~0u, ~0u, ~0u, ~0u);
-            if (base_m) m = and4(m, __ldg(base_m + w));
-            if (base_i) m = and4(m, __ldg(base_i + w));
-            if (rs) m = and4(m, __ldg(rs + w));
-            if (ri) m = and4(m, __ldg(ri + w));
-            sm4[r * nw4 + w] = m;
-        }
+    if (threadIdx.x < kLop3Rows && (int)threadIdx.x < t.nr) {
+        const RowDesc rd = a.rows[j.row_off + t.r0 + threadIdx.x];
+        rsrc[threadIdx.x][0] = rd.slot >= 0 ? reinterpret_cast<const uint4*>(a.masks + (int64_t)rd.slot * W) : nullptr;
+        rsrc[threadIdx.x][1] = rd.item >= 0 ? reinterpret_cast<const uint4*>(a.bitmap + (int64_t)rd.item * W) : nullptr;
     }
-    __syncthreads();
-    // 2. one warp per column: stream the column row through every staged row
+    const uint4* base_m = j.base_slot >= 0 ? reinterpret_cast<const uint4*>(a.masks + (int64_t)j.base_slot * W) : nullptr;
+    const uint4* base_i = j.base_item >= 0 ? reinterpret_cast<const uint4*>(a.bitmap + (int64_t)j.base_item * W) : nullptr;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int c = t.c0 + warp; c < t.c1; c += 8) {
-        const int32_t col = a.cols[j.col_off + c];
-        const uint4* cp = col >= 0 ? reinterpret_cast<const uint4*>(a.bitmap + (int64_t)col * W + t.w0) : nullptr;
-        uint32_t acc[kLop3Rows];
-#pragma unroll
-        for (int r = 0; r < kLop3Rows; r++) acc[r] = 0;
-        for (int w = lane; w < nw4; w += 32) {
-            const uint4 v = cp ? __ldg(cp + w) : make_uint4(~0u, ~0u, ~0u, ~0u);
-#pragma unroll
-            for (int r = 0; r < kLop3Rows; r++)
-                if (r < t.nr) acc[r] += popc4(and4(sm4[r * nw4 + w], v));
+    for (int cw = t.w0; cw < t.w1; cw += kLop3Chunk) {
+        const int w4b = cw >> 2;
+        const int nw4 = (min(t.w1, cw + kLop3Chunk) - cw) >> 2;
+        __syncthreads();   // rsrc visible; previous chunk's readers done
+        // 1. stage the tile's row masks for this word chunk
+        for (int r = 0; r < t.nr; r++) {
+            const uint4* rs = rsrc[r][0];
+            const uint4* ri = rsrc[r][1];
+            for (int w = threadIdx.x; w < nw4; w += blockDim.x) {
+                uint4 m = make_uint4(~0u, ~0u, ~0u, ~0u);
+                if (base_m) m = and4(m, __ldg(base_m + w4b + w));
+                if (base_i) m = and4(m, __ldg(base_i + w4b + w));
+                if (rs) m = and4(m, __ldg(rs + w4b + w));
+                if (ri) m = and4(m, __ldg(ri + w4b + w));
+                sm4[r * nw4 + w] = m;
+            }
         }
+        __syncthreads();
+        // 2. one warp per column: stream the column row through every staged row
+        for (int c = t.c0 + warp; c < t.c1; c += 8) {
+            const int32_t col = a.cols[j.col_off + c];
+            const uint4* cp = col >= 0 ? reinterpret_cast<const uint4*>(a.bitmap + (int64_t)col * W) + w4b : nullptr;
+            uint32_t acc[kLop3Rows];
 #pragma unroll
-        for (int r = 0; r < kLop3Rows; r++) {
-            if (r >= t.nr) break;
-            uint32_t v = acc[r];
+            for (int r = 0; r < kLop3Rows; r++) acc[r] = 0;
+            for (int w = lane; w < nw4; w += 32) {
+                const uint4 v = cp ? __ldg(cp + w) : make_uint4(~0u, ~0u, ~0u, ~0u);
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-            if (lane == 0 && v) atomicAdd(a.out + j.out_off + (int64_t)(t.r0 + r) * j.n_cols + c, (int32_t)v);
+                for (int r = 0; r < kLop3Rows; r++)
+                    if (r < t.nr) acc[r] += popc4(and4(sm4[r * nw4 + w], v));
+            }
+#pragma unroll
+            for (int r = 0; r < kLop3Rows; r++) {
+                if (r >= t.nr) break;
+                uint32_t v = acc[r];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+                if (lane == 0 && v) atomicAdd(a.out + j.out_off + (int64_t)(t.r0 + r) * j.n_cols + c, (int32_t)v);
+            }
         }
     }
 }

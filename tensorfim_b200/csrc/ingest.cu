@@ -216,6 +216,7 @@ int ingest_csr(tfim_ctx* c, const int64_t* h_off, const int32_t* h_items, int64_
     TFIM_CHECK(nnz >= 0, TFIM_E_INVALID, "row_offsets[n_rows] is negative");
 
     DevBuf d_off, d_items, d_stats, d_freq, d_map, d_flag, d_idx, d_tmp;
+    for (DevBuf* b : {&d_off, &d_items, &d_stats, &d_freq, &d_map, &d_flag, &d_idx, &d_tmp}) b->stream = s;
     int rc = TFIM_OK;
     ScanStats hs{};
     std::vector<int32_t> freq;
@@ -334,12 +335,9 @@ int ingest_csr(tfim_ctx* c, const int64_t* h_off, const int32_t* h_items, int64_
     I.trans_len_red_max = n_red > 0 ? hs.red_max : 0;
     I.trans_len_red_mean = (double)hs.red_sum / (double)n_red;   // 0/0 -> nan, as the reference
     c->red_pair_work = (double)hs.red_sq_sum;
-    if (cudaMalloc(&c->d_red_off, (size_t)(n_red + 1) * 8) != cudaSuccess ||
-        cudaMalloc(&c->d_red_items, (size_t)std::max<int64_t>(n_red_items, 1) * 4) != cudaSuccess) {
-        cudaGetLastError();
-        set_error("reduced transaction list allocation failed");
-        return done(TFIM_E_NOMEM);
-    }
+    if ((rc = dev_alloc((void**)&c->d_red_off, (size_t)(n_red + 1) * 8, s)) ||
+        (rc = dev_alloc((void**)&c->d_red_items, (size_t)std::max<int64_t>(n_red_items, 1) * 4, s)))
+        return done(rc);
     c->n_red_items = n_red_items;
     cudaMemcpyAsync(c->d_red_off + n_red, &n_red_items, 8, cudaMemcpyHostToDevice, s);
     if (n_red > 0)
@@ -351,12 +349,7 @@ int ingest_csr(tfim_ctx* c, const int64_t* h_off, const int32_t* h_items, int64_
     c->W = words_for_bits(n_red);
     I.words_per_row = (int32_t)c->W;
     const size_t bm_bytes = (size_t)std::max<int32_t>(n_dense, 1) * (size_t)std::max<int64_t>(c->W, 1) * 4;
-    if (cudaMalloc(&c->d_bitmap, bm_bytes) != cudaSuccess) {
-        cudaGetLastError();
-        c->d_bitmap = nullptr;
-        set_error("bitmap allocation of %zu bytes failed", bm_bytes);
-        return done(TFIM_E_NOMEM);
-    }
+    if ((rc = dev_alloc((void**)&c->d_bitmap, bm_bytes, s))) return done(rc);
     cudaMemsetAsync(c->d_bitmap, 0, bm_bytes, s);
     if (n_red > 0)
         k_scatter_bits<<<grid_for(n_red), 256, 0, s>>>(c->d_red_off, c->d_red_items, n_red, c->d_bitmap, c->W);
@@ -382,12 +375,7 @@ int ingest_bitmap(tfim_ctx* c, const uint32_t* rows, int32_t n_rows, int64_t n_b
     c->info.trans_num_reduced = n_bits;
     c->info.words_per_row = (int32_t)c->W;
     const size_t bytes = (size_t)n_rows * (size_t)c->W * 4;
-    if (cudaMalloc(&c->d_bitmap, bytes) != cudaSuccess) {
-        cudaGetLastError();
-        c->d_bitmap = nullptr;
-        set_error("bitmap allocation of %zu bytes failed", bytes);
-        return TFIM_E_NOMEM;
-    }
+    TFIM_TRY(dev_alloc((void**)&c->d_bitmap, bytes, c->stream));
     TFIM_CUDA(cudaMemsetAsync(c->d_bitmap, 0, bytes, c->stream));
     TFIM_CUDA(cudaMemcpy2DAsync(c->d_bitmap, (size_t)c->W * 4, rows, (size_t)src_w * 4, (size_t)src_w * 4, n_rows,
                                 cudaMemcpyHostToDevice, c->stream));

@@ -62,11 +62,11 @@ struct SlotPool {
         if (need <= cap) return TFIM_OK;
         int32_t ncap = std::max<int32_t>(need, std::max<int32_t>(64, cap * 2));
         DevBuf nb;
+        nb.stream = c->stream;
         TFIM_TRY(nb.reserve((size_t)ncap * (size_t)c->W * 4));
         if (c->d_masks.p && cap > 0)
             TFIM_CUDA(cudaMemcpyAsync(nb.p, c->d_masks.p, (size_t)cap * (size_t)c->W * 4, cudaMemcpyDeviceToDevice, c->stream));
-        TFIM_CUDA(cudaStreamSynchronize(c->stream));
-        c->d_masks.release();
+        c->d_masks.release();   // stream-ordered: after the copy
         c->d_masks = nb;
         cap = ncap;
         return TFIM_OK;
@@ -90,16 +90,16 @@ struct SlotPool {
 // Tile builders --------------------------------------------------------------------------
 // `upper`: the job's rows and columns are the same list; only tiles holding some (i, j>=i)
 // are emitted and the mirror pass fills the rest.
-void tiles_lop3(int32_t job, int32_t nr, int32_t nc, int64_t W, std::vector<TileDesc>& out, bool upper = false) {
-    const int64_t chunk = std::min<int64_t>(W, kLop3Chunk);
+void tiles_lop3(int32_t job, int32_t nr, int32_t nc, int64_t W, int64_t wslice, std::vector<TileDesc>& out,
+                bool upper = false) {
     for (int32_t r0 = 0; r0 < nr; r0 += kLop3Rows)
         for (int32_t c0 = 0; c0 < nc; c0 += 64)
-            for (int64_t w0 = 0; w0 < W; w0 += chunk) {
+            for (int64_t w0 = 0; w0 < W; w0 += wslice) {
                 if (upper && std::min(nc, c0 + 64) <= r0) continue;
                 TileDesc t;
                 t.job = job; t.r0 = r0; t.nr = std::min(kLop3Rows, nr - r0);
                 t.c0 = c0; t.c1 = std::min(nc, c0 + 64);
-                t.w0 = (int32_t)w0; t.w1 = (int32_t)std::min<int64_t>(W, w0 + chunk);
+                t.w0 = (int32_t)w0; t.w1 = (int32_t)std::min<int64_t>(W, w0 + wslice);
                 t.pad = 0;
                 out.push_back(t);
             }
@@ -191,6 +191,18 @@ struct WaveRunner {
         for (size_t j = 0; j < w.jobs.size(); j++)
             if (w.use_b1[j] && !((int32_t)j == w.top_job && w.top_mode == 2))
                 base_b1 += (int64_t)((w.jobs[j].n_rows + kB1Rows - 1) / kB1Rows) * ((w.jobs[j].n_cols + kB1Cols - 1) / kB1Cols);
+        // word slices of CUDA-core tiles: whole rows when the wave has many tiles already
+        int64_t base_l3 = 0;
+        for (size_t j = 0; j < w.jobs.size(); j++)
+            if (!w.use_b1[j] && !((int32_t)j == w.top_job && w.top_mode == 2))
+                base_l3 += (int64_t)((w.jobs[j].n_rows + kLop3Rows - 1) / kLop3Rows) * ((w.jobs[j].n_cols + 63) / 64);
+        int64_t wslice = W;
+        if (base_l3 > 0) {
+            const int64_t want = 8LL * sm_count;
+            int64_t ks = std::max<int64_t>(1, (want + base_l3 - 1) / base_l3);
+            ks = std::min<int64_t>(ks, std::max<int64_t>(1, W / 256));
+            wslice = ((W / 64 + ks - 1) / ks) * 64;
+        }
         int64_t kslice = W;
         if (base_b1 > 0) {
             const int64_t want = 4LL * sm_count;
@@ -213,7 +225,7 @@ struct WaveRunner {
             const bool top = (int32_t)j == w.top_job;
             if (top && w.top_mode == 2) continue;
             if (w.use_b1[j]) tiles_b1((int32_t)j, w.jobs[j].n_rows, w.jobs[j].n_cols, W, kslice, t_b1, top);
-            else tiles_lop3((int32_t)j, w.jobs[j].n_rows, w.jobs[j].n_cols, W, t_l3, top);
+            else tiles_lop3((int32_t)j, w.jobs[j].n_rows, w.jobs[j].n_cols, W, wslice, t_l3, top);
         }
         Packer pk;
         const size_t o_jobs = pk.add(w.jobs.data(), w.jobs.size() * sizeof(JobDesc));
@@ -357,7 +369,11 @@ void free_engine(EngineState* e) {
 namespace {
 
 EngineState& engine_state(tfim_ctx* c) {
-    if (!c->engine) c->engine = new EngineState();
+    if (!c->engine) {
+        c->engine = new EngineState();
+        for (DevBuf* b : {&c->engine->wr.d_desc, &c->engine->wr.d_counts, &c->engine->wr.d_entries, &c->engine->wr.d_rowinfo})
+            b->stream = c->stream;
+    }
     c->engine->wr.c = c;
     c->engine->wr.reset_counters();
     c->engine->pool.reset(c);
@@ -671,9 +687,27 @@ int mine_batched(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* st) {
                     ch.slot = s;
                     ch.item = -1;
                 }
-                // lookahead on head + tail
+                // lookahead on head + tail, only when every pair of tail items is frequent
+                // with P (a necessary condition, read from P's counted rows)
                 const int32_t list_len = (int32_t)ch.T.size() + (ch.item >= 0 ? 1 : 0);
-                if (lookahead && ch.T.size() >= 2 && list_len <= kMaxListLen) {
+                bool try_look = lookahead && ch.T.size() >= 2 && list_len <= kMaxListLen;
+                if (try_look) {
+                    for (size_t a = 0; a < tail.size() && try_look; a++) {
+                        const int32_t ra = tail[a].first;   // F index < |T(P)|: a row of P's family
+                        if (ra < pc.r0 || ra >= pc.r1) continue;   // row not in this wave: no filter
+                        const int2 rinfo = wr.row_info[job_row_base[pc.job] + (ra - pc.r0)];
+                        const Entry* eb = wr.entries.data() + rinfo.x;
+                        const Entry* ee = eb + rinfo.y;
+                        for (size_t b = 0; b < tail.size(); b++) {
+                            if (b == a) continue;
+                            const int32_t cb = tail[b].first;
+                            const Entry* it = std::lower_bound(eb, ee, cb, [](const Entry& x, int32_t v) { return x.col < v; });
+                            if (it == ee || it->col != cb) { try_look = false; break; }
+                        }
+                    }
+                    if (!try_look) st->lookaheads_skipped++;
+                }
+                if (try_look) {
                     int32_t ls = 0;
                     TFIM_TRY(pool.alloc(c, &ls));
                     MatDesc m;

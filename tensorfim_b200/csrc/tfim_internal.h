@@ -49,10 +49,20 @@ inline int64_t words_for_bits(int64_t bits) {
 
 constexpr int kMaxListLen = 64;   // longest item list one counted row may AND
 
-// A device buffer that grows on demand and is freed with the context.
+// Device memory comes from one stream-ordered pool per device that keeps freed blocks
+// cached (up to a release threshold), so opening and closing contexts or growing
+// buffers does not go back to the driver; pinned host staging comes from a process-wide
+// cache of blocks.
+int dev_alloc(void** p, size_t bytes, cudaStream_t s);
+void dev_free(void* p, cudaStream_t s);
+void* pinned_alloc(size_t bytes, size_t* got);
+void pinned_free(void* p, size_t bytes);
+
+// A device buffer that grows on demand (stream-ordered on `stream`), freed with its owner.
 struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
+    cudaStream_t stream = nullptr;
     int reserve(size_t need);
     void release();
     template <typename T> T* as() const { return reinterpret_cast<T*>(p); }

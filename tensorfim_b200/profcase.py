@@ -1,0 +1,37 @@
+"""One mine of a seeded benchmark database, for profiler captures.
+
+    python -m tensorfim_b200.profcase --cfg 4 --scale 0.25 --counter tensor [--engine batched] [--top auto]
+
+Generates the configuration's database (tensorfim_b200.synth) at the given row scale,
+builds it on cuda:0 and mines it once; prints the MFI count and the engine statistics.
+"""
+import argparse
+import json
+
+from . import synth
+from .engine import Database
+
+MINSUP = {1: 0.10, 2: 0.90, 3: 0.85, 4: 0.0005, 5: 0.70}
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--cfg", type=int, default=4)
+    ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--minsup", type=float, default=None)
+    ap.add_argument("--engine", default="batched")
+    ap.add_argument("--counter", default="auto")
+    ap.add_argument("--top", default="auto")
+    ap.add_argument("--repeat", type=int, default=1)
+    a = ap.parse_args()
+    kw = {"scale": a.scale} if a.cfg != 3 else {"scale": a.scale, "replicas": 1}
+    db0 = synth.generate(a.cfg, **kw)
+    minsup = a.minsup if a.minsup is not None else MINSUP[a.cfg]
+    with Database.from_csr(db0.offsets, db0.items, minsup) as db:
+        for _ in range(a.repeat):
+            r = db.mine(engine=a.engine, counter=a.counter, top=a.top)
+        print(json.dumps({"mfis": len(r.mfis), "info": db.info, "stats": r.stats}))
+
+
+if __name__ == "__main__":
+    main()
