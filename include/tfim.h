@@ -127,6 +127,27 @@ TFIM_API int tfim_count_wave_device(tfim_ctx* ctx, const int32_t* d_item_lists, 
                            int32_t b, int32_t max_len, int32_t min_count,
                            int32_t* d_counts_out, int32_t* d_nfreq_out, void* stream);
 
+/*
+ * Allocation-free form of tfim_count_wave_device, for callers that cannot allocate GPU
+ * memory (an allocator that owns the whole device, work recorded while a stream is being
+ * captured, code that only holds pointers it was handed).  It needs no context: the
+ * caller passes a device bitmap (n_counted rows of words_per_row uint32 words, 16-byte
+ * aligned, words_per_row a multiple of 4, bits past the last transaction zero), the
+ * device item lists and offsets, and the outputs; the result contract is
+ * tfim_count_wave's.  The per-node prefix masks go to a fixed 16 MiB device array
+ * inside the library (held on every device that loads it, until exit): a call needing
+ * more than b * words_per_row * 4 = 16 MiB is rejected with TFIM_E_INVALID, and so is
+ * b > 65535.  The array is shared by all calls and keeps the last call's contents, so
+ * calls that overlap on the GPU race.  The first call on a device looks the array's
+ * address up (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture.  Item ids are not range-checked (they are in device memory).
+ * Enqueued on `stream` (NULL = the legacy default stream); returns after enqueueing.
+ * No counterpart in the reference.
+ */
+TFIM_API int tfim_count_wave_noalloc(const uint32_t* d_bitmap, int64_t words_per_row, int32_t n_counted,
+                                     const int32_t* d_item_lists, const int64_t* d_list_offsets, int32_t b,
+                                     int32_t min_count, int32_t* d_counts_out, int32_t* d_nfreq_out, void* stream);
+
 /* mining engines */
 #define TFIM_ENGINE_PLAIN    0   /* the reference's search, one counted node per launch */
 #define TFIM_ENGINE_BATCHED  1   /* pruned search counted in waves of families */

@@ -33,6 +33,7 @@ EXPORTS = [
     "tfim_dense_to_orig", "tfim_dense_freq", "tfim_count_wave", "tfim_set_counter",
     "tfim_count_wave_device", "tfim_mine_opts_default", "tfim_mine", "tfim_num_mfis",
     "tfim_mfi_item_total", "tfim_get_mfis", "tfim_write_results", "tfim_close",
+    "tfim_count_wave_noalloc",
 ]
 
 
@@ -99,6 +100,7 @@ def lib() -> C.CDLL:
     L.tfim_count_wave.argtypes = [p, p, p, i32, i32, p, p]
     L.tfim_set_counter.argtypes = [p, i32]
     L.tfim_count_wave_device.argtypes = [p, p, p, i32, i32, i32, p, p, p]
+    L.tfim_count_wave_noalloc.argtypes = [p, i64, i32, p, p, i32, i32, p, p, p]
     L.tfim_mine_opts_default.argtypes = [P(MineOpts)]
     L.tfim_mine_opts_default.restype = None
     L.tfim_mine.argtypes = [p, P(MineOpts), P(MineStats)]
