@@ -156,11 +156,13 @@ typedef struct {
     int32_t engine;        /* TFIM_ENGINE_* */
     int32_t counter;       /* TFIM_COUNTER_* */
     int32_t wave_cap;      /* max family rows per wave; 0 = tuned default */
-    int32_t lookahead;     /* 0 off, 1 on (head-union-tail check), 2 learned proposal */
+    int32_t lookahead;     /* 0 off, 1 every node that passes the tail-pair filter,
+                              2 learned proposal (tfim_set_proposal), 3 every node (no filter) */
     int32_t use_graphs;    /* replay wave launches as CUDA graphs when possible */
     int32_t top_counter;   /* family of the empty prefix: 0 by cost model, 1 bitmap Gram,
                               2 pair co-occurrence over the reduced transaction list */
-    int32_t reserved[10];
+    int32_t log_lookahead; /* 1: log features and outcomes of every lookahead issued */
+    int32_t reserved[9];
 } tfim_mine_opts;
 
 typedef struct {
@@ -210,6 +212,43 @@ TFIM_API int tfim_write_results(const tfim_ctx* ctx, const char* trans_set_file,
                        double preprocessing_s, double computation_s);
 
 TFIM_API void tfim_close(tfim_ctx* ctx);
+
+/* ------------------------------------------------------------------------------------
+ * Learned lookahead proposal (no counterpart in the reference, which has no learned part).
+ * A 32 -> 64 -> 64 -> 1 MLP (ReLU, ReLU, sigmoid), BF16 weights, FP32 accumulation,
+ * trained and evaluated by the library's own CUDA kernels.  It scores a search node
+ * (features: depth, head size, tail size, head support, tail-item supports, prefix
+ * density, ...) with the probability that head + tail is frequent; the batched engine
+ * issues the head-union-tail lookahead first only for nodes it scores high.  It decides
+ * ordering and which exact checks run first only: results never depend on it.
+ * Parameters (tfim_mlp_num_params() floats): W1[64][32], b1[64], W2[64][64], b2[64],
+ * W3[64], b3.
+ */
+typedef struct tfim_mlp tfim_mlp;
+#define TFIM_MLP_FEATURES 32
+TFIM_API int tfim_mlp_create(int32_t device, uint64_t seed, tfim_mlp** out);
+TFIM_API int tfim_mlp_num_params(void);
+TFIM_API int tfim_mlp_set_params(tfim_mlp* mlp, const float* params);
+TFIM_API int tfim_mlp_get_params(const tfim_mlp* mlp, float* params);
+/* probs[i] = sigmoid(MLP(feats[i*32 .. i*32+32))) */
+TFIM_API int tfim_mlp_predict(tfim_mlp* mlp, const float* feats, int64_t n, float* probs);
+/* gradient of mean_i w_i * BCE(probs_i, labels_i) (w_i = pos_weight when label 1) with
+ * respect to the FP32 parameters, through the BF16 forward pass; loss may be NULL */
+TFIM_API int tfim_mlp_grad(tfim_mlp* mlp, const float* feats, const float* labels, int64_t n, float pos_weight,
+                           float* grads, float* loss);
+/* Adam over minibatches in the given order, on the GPU */
+TFIM_API int tfim_mlp_train(tfim_mlp* mlp, const float* feats, const float* labels, int64_t n, int32_t epochs,
+                            int32_t batch, float lr, float pos_weight, float weight_decay, float* final_loss);
+TFIM_API void tfim_mlp_free(tfim_mlp* mlp);
+
+/* Attach a proposal network to a context (not owned; NULL detaches).  With
+ * tfim_mine_opts.lookahead == 2 the engine issues a lookahead only for nodes scored
+ * >= threshold. */
+TFIM_API int tfim_set_proposal(tfim_ctx* ctx, tfim_mlp* mlp, float threshold);
+/* Lookahead outcomes logged by the last tfim_mine run with opts.log_lookahead = 1:
+ * feats (n x 32) and labels (1 = head + tail was frequent).  Returns the number of
+ * records (copies at most cap of them); negative on error. */
+TFIM_API int64_t tfim_lookahead_log(const tfim_ctx* ctx, float* feats, float* labels, int64_t cap);
 
 #ifdef __cplusplus
 }

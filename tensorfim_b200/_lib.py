@@ -34,6 +34,8 @@ EXPORTS = [
     "tfim_count_wave_device", "tfim_mine_opts_default", "tfim_mine", "tfim_num_mfis",
     "tfim_mfi_item_total", "tfim_get_mfis", "tfim_write_results", "tfim_close",
     "tfim_count_wave_noalloc",
+    "tfim_mlp_create", "tfim_mlp_num_params", "tfim_mlp_set_params", "tfim_mlp_get_params", "tfim_mlp_predict",
+    "tfim_mlp_grad", "tfim_mlp_train", "tfim_mlp_free", "tfim_set_proposal", "tfim_lookahead_log",
 ]
 
 
@@ -61,7 +63,7 @@ class DbInfo(C.Structure):
 class MineOpts(C.Structure):
     _fields_ = [("engine", C.c_int32), ("counter", C.c_int32), ("wave_cap", C.c_int32),
                 ("lookahead", C.c_int32), ("use_graphs", C.c_int32), ("top_counter", C.c_int32),
-                ("reserved", C.c_int32 * 10)]
+                ("log_lookahead", C.c_int32), ("reserved", C.c_int32 * 9)]
 
 
 class MineStats(C.Structure):
@@ -112,6 +114,17 @@ def lib() -> C.CDLL:
     L.tfim_write_results.argtypes = [p, C.c_char_p, C.c_char_p, C.c_double, C.c_double]
     L.tfim_close.argtypes = [p]
     L.tfim_close.restype = None
+    L.tfim_mlp_create.argtypes = [i32, C.c_uint64, P(p)]
+    L.tfim_mlp_set_params.argtypes = [p, p]
+    L.tfim_mlp_get_params.argtypes = [p, p]
+    L.tfim_mlp_predict.argtypes = [p, p, i64, p]
+    L.tfim_mlp_grad.argtypes = [p, p, p, i64, C.c_float, p, p]
+    L.tfim_mlp_train.argtypes = [p, p, p, i64, i32, i32, C.c_float, C.c_float, C.c_float, p]
+    L.tfim_mlp_free.argtypes = [p]
+    L.tfim_mlp_free.restype = None
+    L.tfim_set_proposal.argtypes = [p, p, C.c_float]
+    L.tfim_lookahead_log.argtypes = [p, p, p, i64]
+    L.tfim_lookahead_log.restype = i64
     for name in EXPORTS:
         getattr(L, name)   # raises AttributeError if an export is missing
     _lib = L

@@ -305,6 +305,25 @@ int tfim_mine(tfim_ctx* c, const tfim_mine_opts* opts, tfim_mine_stats* stats) {
     return TFIM_OK;
 }
 
+int tfim_set_proposal(tfim_ctx* c, tfim_mlp* mlp, float threshold) {
+    TFIM_CHECK(c, TFIM_E_INVALID, "null context");
+    c->proposal = mlp;
+    c->proposal_threshold = threshold;
+    return TFIM_OK;
+}
+
+int64_t tfim_lookahead_log(const tfim_ctx* c, float* feats, float* labels, int64_t cap) {
+    if (!c) { set_error("null context"); return -TFIM_E_INVALID; }
+    const int64_t n = (int64_t)c->la_labels.size();
+    const int64_t k = std::min<int64_t>(n, std::max<int64_t>(cap, 0));
+    if (k > 0) {
+        if (!feats || !labels) { set_error("null buffers"); return -TFIM_E_INVALID; }
+        memcpy(feats, c->la_feats.data(), (size_t)k * 32 * sizeof(float));
+        memcpy(labels, c->la_labels.data(), (size_t)k * sizeof(float));
+    }
+    return n;
+}
+
 int64_t tfim_num_mfis(const tfim_ctx* c) { return c && c->mined ? (int64_t)c->mfi_items.size() : -1; }
 
 int64_t tfim_mfi_item_total(const tfim_ctx* c) {

@@ -368,6 +368,51 @@ void free_engine(EngineState* e) {
 
 namespace {
 
+// Features of a lookahead candidate (the learned proposal's input, 32 floats).
+void lookahead_features(float* f, int head_n, const std::vector<std::pair<int32_t, int32_t>>& tail, int nF, int32_t supc,
+                        int32_t minc, int64_t nbits, int n_eq, double pair_frac, int parent_tail, int row, bool top_child) {
+    for (int q = 0; q < 32; q++) f[q] = 0.f;
+    const int k = (int)tail.size();
+    double mn = 1e30, mn2 = 1e30, mx = 0, sum = 0, sum2 = 0, logprod = 0;
+    int gt90 = 0, gt99 = 0;
+    for (auto& pr : tail) {
+        const double r = (double)pr.second / (double)supc;
+        if (r < mn) { mn2 = mn; mn = r; } else if (r < mn2) mn2 = r;
+        mx = std::max(mx, r);
+        sum += r;
+        sum2 += r * r;
+        logprod += std::log(std::max(r, 1e-12));
+        gt90 += r > 0.9;
+        gt99 += r > 0.99;
+    }
+    const double mean = k ? sum / k : 0, var = k ? std::max(0.0, sum2 / k - mean * mean) : 0;
+    const double minc_d = std::max<int32_t>(1, minc);
+    f[0] = head_n / 16.f;
+    f[1] = k / 32.f;
+    f[2] = nF / 64.f;
+    f[3] = (float)((double)supc / (double)std::max<int64_t>(1, nbits));
+    f[4] = (float)(std::log2(1.0 + supc) / 24.0);
+    f[5] = (float)mn;
+    f[6] = (float)mean;
+    f[7] = (float)mx;
+    f[8] = (float)(std::min(mn * supc / minc_d, 8.0) / 8.0);
+    f[9] = (float)std::exp(logprod);
+    f[10] = (float)(std::max(-8.0, std::min(8.0, logprod + std::log(supc / minc_d))) / 8.0);
+    f[11] = (float)pair_frac;
+    f[12] = (nF - k) / 64.f;
+    f[13] = (float)(minc_d / (double)std::max<int64_t>(1, nbits));
+    f[14] = (float)(std::min(supc / minc_d, 64.0) / 64.0);
+    f[15] = (float)std::sqrt(var);
+    f[16] = (float)(k > 1 ? mn2 : mn);
+    f[17] = k ? (float)gt90 / k : 0.f;
+    f[18] = k ? (float)gt99 / k : 0.f;
+    f[19] = (float)(std::log2(1.0 + k) / 6.0);
+    f[20] = n_eq / 8.f;
+    f[21] = parent_tail / 64.f;
+    f[22] = (float)row / (float)std::max(1, parent_tail);
+    f[23] = top_child ? 1.f : 0.f;
+}
+
 EngineState& engine_state(tfim_ctx* c) {
     if (!c->engine) {
         c->engine = new EngineState();
@@ -490,12 +535,24 @@ int mine_batched(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* st) {
         int32_t fam;                        // family it decides
         int32_t slot;                       // mask of head + tail
         std::vector<int32_t> cols;          // F \ T, then -1 (self)
+        int64_t log = -1;                   // index into the outcome log
     };
+    struct Cand {                           // a family that may get a lookahead
+        int32_t fam;
+        int32_t src_slot, src_item, t;      // its mask = masks[src_slot] & B[src_item] & B[t]
+        float feat[32];
+    };
+    std::vector<Cand> cands;
+    std::vector<float> probs;
+    c->la_feats.clear();
+    c->la_labels.clear();
     std::deque<Fam> fams;   // stable references while children are appended
     std::vector<int32_t> stack;             // family ids, top = back
     std::vector<Look> looks_pending;        // issued with the next wave
     const int32_t wave_cap = o->wave_cap > 0 ? o->wave_cap : 4096;
-    const bool lookahead = o->lookahead != 0;
+    const int32_t la_mode = o->lookahead;   // 0 off, 1 filtered, 2 learned, 3 every node
+    const bool lookahead = la_mode != 0;
+    TFIM_CHECK(la_mode != 2 || c->proposal, TFIM_E_STATE, "lookahead mode 2 needs a proposal network (tfim_set_proposal)");
 
     // top-level family: P = {}, F = T = counted items that are frequent by bitmap support
     {
@@ -608,6 +665,7 @@ int mine_batched(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* st) {
                 else ext = true;
             }
             pool.release(L.slot);
+            if (L.log >= 0) c->la_labels[L.log] = self >= 0 ? 1.f : 0.f;
             if (self >= 0) {   // head + tail is frequent: it decides the whole subtree
                 st->lookahead_hits++;
                 if (!ext) {
@@ -687,52 +745,38 @@ int mine_batched(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* st) {
                     ch.slot = s;
                     ch.item = -1;
                 }
-                // lookahead on head + tail, only when every pair of tail items is frequent
-                // with P (a necessary condition, read from P's counted rows)
-                const int32_t list_len = (int32_t)ch.T.size() + (ch.item >= 0 ? 1 : 0);
-                bool try_look = lookahead && ch.T.size() >= 2 && list_len <= kMaxListLen;
-                if (try_look) {
-                    for (size_t a = 0; a < tail.size() && try_look; a++) {
+                // lookahead on head + tail.  Filter: every pair of tail items must be frequent
+                // with P (a necessary condition, read from P's counted rows).
+                const int32_t list_len = (int32_t)ch.T.size() + 1 + (P.item >= 0 ? 1 : 0);
+                if (lookahead && ch.T.size() >= 2 && list_len <= kMaxListLen) {
+                    int64_t pairs = 0, pairs_ok = 0;
+                    bool filtered = false;
+                    for (size_t a = 0; a < tail.size(); a++) {
                         const int32_t ra = tail[a].first;   // F index < |T(P)|: a row of P's family
-                        if (ra < pc.r0 || ra >= pc.r1) continue;   // row not in this wave: no filter
+                        if (ra < pc.r0 || ra >= pc.r1) continue;   // row not in this wave: unknown
                         const int2 rinfo = wr.row_info[job_row_base[pc.job] + (ra - pc.r0)];
                         const Entry* eb = wr.entries.data() + rinfo.x;
                         const Entry* ee = eb + rinfo.y;
-                        for (size_t b = 0; b < tail.size(); b++) {
-                            if (b == a) continue;
+                        for (size_t b = a + 1; b < tail.size(); b++) {
                             const int32_t cb = tail[b].first;
                             const Entry* it = std::lower_bound(eb, ee, cb, [](const Entry& x, int32_t v) { return x.col < v; });
-                            if (it == ee || it->col != cb) { try_look = false; break; }
+                            pairs++;
+                            if (it != ee && it->col == cb) pairs_ok++;
+                            else filtered = true;
                         }
                     }
-                    if (!try_look) st->lookaheads_skipped++;
-                }
-                if (try_look) {
-                    int32_t ls = 0;
-                    TFIM_TRY(pool.alloc(c, &ls));
-                    MatDesc m;
-                    m.dst = ls; m.src = -1; m.off = (int32_t)pending_mat_items.size(); m.n = 0;
-                    if (ch.slot >= 0) {
-                        // the child's mask is materialised in the same launch: derive from P instead
-                        m.src = P.slot;
-                        if (P.item >= 0) { pending_mat_items.push_back(P.item); m.n++; }
-                        pending_mat_items.push_back(t); m.n++;
+                    if (filtered && la_mode != 3) {
+                        st->lookaheads_skipped++;
                     } else {
-                        pending_mat_items.push_back(ch.item); m.n++;
-                    }
-                    for (int32_t x : ch.T) { pending_mat_items.push_back(x); m.n++; }
-                    if (m.n <= kMaxListLen) {
-                        pending_mats.push_back(m);
-                        Look L;
-                        L.fam = (int32_t)fams.size();
-                        L.slot = ls;
-                        for (size_t q = ch.T.size(); q < ch.F.size(); q++) L.cols.push_back(ch.F[q]);
-                        L.cols.push_back(-1);
-                        looks_pending.push_back(std::move(L));
-                        ch.waiting = true;
-                    } else {
-                        pending_mat_items.resize(m.off);
-                        pool.release(ls);
+                        Cand cd;
+                        cd.fam = (int32_t)fams.size();
+                        cd.src_slot = P.slot;
+                        cd.src_item = P.item;
+                        cd.t = t;
+                        lookahead_features(cd.feat, (int)ch.head.size(), tail, (int)ch.F.size(), supc, minc, c->n_bits,
+                                           (int)eq.size(), pairs ? (double)pairs_ok / (double)pairs : 1.0, nT, i,
+                                           P.slot < 0 && P.item < 0);
+                        cands.push_back(cd);
                     }
                 }
                 new_fams.push_back((int32_t)fams.size());
@@ -747,6 +791,46 @@ int mine_batched(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* st) {
                 P2.T.clear(); P2.T.shrink_to_fit();
                 P2.head.clear(); P2.head.shrink_to_fit();
             }
+        }
+        // lookahead decisions for this wave's candidates
+        if (!cands.empty()) {
+            probs.assign(cands.size(), 1.f);
+            if (la_mode == 2) {
+                std::vector<float> feats(cands.size() * 32);
+                for (size_t q = 0; q < cands.size(); q++) memcpy(&feats[q * 32], cands[q].feat, 32 * sizeof(float));
+                const double tp = now_s();
+                if (tfim_mlp_predict(c->proposal, feats.data(), (int64_t)cands.size(), probs.data()) != TFIM_OK) return TFIM_E_CUDA;
+                st->reserved[0] += (int64_t)((now_s() - tp) * 1e6);   // proposal time, microseconds
+            }
+            for (size_t q = 0; q < cands.size(); q++) {
+                const Cand& cd = cands[q];
+                if (la_mode == 2 && probs[q] < c->proposal_threshold) {
+                    st->lookaheads_skipped++;
+                    continue;
+                }
+                Fam& ch = fams[cd.fam];
+                int32_t ls = 0;
+                TFIM_TRY(pool.alloc(c, &ls));
+                MatDesc m;
+                m.dst = ls; m.src = cd.src_slot; m.off = (int32_t)pending_mat_items.size(); m.n = 0;
+                if (cd.src_item >= 0) { pending_mat_items.push_back(cd.src_item); m.n++; }
+                pending_mat_items.push_back(cd.t); m.n++;
+                for (int32_t x : ch.T) { pending_mat_items.push_back(x); m.n++; }
+                pending_mats.push_back(m);
+                Look L;
+                L.fam = cd.fam;
+                L.slot = ls;
+                for (size_t q2 = ch.T.size(); q2 < ch.F.size(); q2++) L.cols.push_back(ch.F[q2]);
+                L.cols.push_back(-1);
+                if (o->log_lookahead) {
+                    L.log = (int64_t)c->la_labels.size();
+                    c->la_feats.insert(c->la_feats.end(), cd.feat, cd.feat + 32);
+                    c->la_labels.push_back(0.f);
+                }
+                looks_pending.push_back(std::move(L));
+                ch.waiting = true;
+            }
+            cands.clear();
         }
         // children explored first-in-order: push in reverse
         for (auto it = new_fams.rbegin(); it != new_fams.rend(); ++it)

@@ -191,6 +191,11 @@ struct tfim_ctx {
     tfim_mine_stats last_stats{};
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     tfim::EngineState* engine = nullptr;
+    // learned lookahead proposal (not owned) and the outcome log of the last mine
+    tfim_mlp* proposal = nullptr;
+    float proposal_threshold = 0.5f;
+    std::vector<float> la_feats;    // n x 32
+    std::vector<float> la_labels;   // n
 };
 
 namespace tfim {

@@ -74,8 +74,10 @@ class MineResult:
 class Database:
     """A transaction database resident on one GPU (a tfim_ctx)."""
 
-    def __init__(self, handle: C.c_void_p):
+    def __init__(self, handle: C.c_void_p, device: int = 0):
         self._h = handle
+        self._device = device
+        self._proposal = None
         info = _lib.DbInfo()
         check(lib().tfim_db_info_get(self._h, C.byref(info)))
         self.info = info.as_dict()
@@ -87,7 +89,7 @@ class Database:
         items = np.ascontiguousarray(items, dtype=np.int32)
         h = C.c_void_p()
         check(lib().tfim_open_db(_ptr(offsets), _ptr(items), offsets.shape[0] - 1, float(minsup), device, C.byref(h)))
-        return cls(h)
+        return cls(h, device)
 
     @classmethod
     def from_file(cls, path: str, minsup: float, device: int = 0) -> "Database":
@@ -99,7 +101,7 @@ class Database:
         rows = np.ascontiguousarray(rows, dtype=np.uint32)
         h = C.c_void_p()
         check(lib().tfim_open_bitmap(_ptr(rows), rows.shape[0], int(n_bits), int(n_counted), device, C.byref(h)))
-        return cls(h)
+        return cls(h, device)
 
     # -- tables --------------------------------------------------------------------------
     def dense_to_orig(self) -> np.ndarray:
@@ -135,13 +137,38 @@ class Database:
                                            C.c_void_p(stream or None)))
 
     # -- search ----------------------------------------------------------------------------
-    def mine(self, engine: str = "batched", counter: str = "auto", lookahead: bool = True,
-             wave_cap: int = 0, top: str = "auto") -> MineResult:
+    def set_proposal(self, proposal, threshold: float | None = None) -> None:
+        """Attach a learned lookahead proposal (tensorfim_b200.learn.Proposal) or None."""
+        self._proposal = proposal   # keep it alive while attached
+        h = proposal._h if proposal is not None else None
+        thr = threshold if threshold is not None else (proposal.threshold if proposal is not None else 0.5)
+        check(lib().tfim_set_proposal(self._h, h, float(thr)))
+
+    def lookahead_log(self) -> tuple[np.ndarray, np.ndarray]:
+        """Features (n x 32) and outcomes of the lookaheads logged by the last mine."""
+        n = lib().tfim_lookahead_log(self._h, None, None, 0)
+        if n < 0:
+            raise TfimError(-n, lib().tfim_last_error().decode())
+        x = np.zeros((n, 32), np.float32)
+        y = np.zeros(n, np.float32)
+        if n:
+            lib().tfim_lookahead_log(self._h, _ptr(x), _ptr(y), n)
+        return x, y
+
+    def mine(self, engine: str = "batched", counter: str = "auto", lookahead=True,
+             wave_cap: int = 0, top: str = "auto", log_lookahead: bool = False) -> MineResult:
+        """lookahead: False/"off", True/"filtered" (every node passing the exact tail-pair
+        filter), "learned" (the attached proposal, or the shipped weights), "all"."""
         o = _lib.MineOpts()
         lib().tfim_mine_opts_default(C.byref(o))
         o.engine = ENGINES[engine]
         o.counter = COUNTERS[counter]
-        o.lookahead = int(lookahead)
+        la = {False: 0, True: 1, "off": 0, "filtered": 1, "learned": 2, "all": 3}[lookahead]
+        if la == 2 and getattr(self, "_proposal", None) is None:
+            from .learn import Proposal
+            self.set_proposal(Proposal.load(device=self._device))
+        o.lookahead = la
+        o.log_lookahead = int(log_lookahead)
         o.wave_cap = int(wave_cap)
         o.top_counter = {"auto": 0, "bitmap": 1, "pairs": 2}[top]
         st = _lib.MineStats()
@@ -162,6 +189,7 @@ class Database:
         if self._h:
             lib().tfim_close(self._h)
             self._h = None
+        self._proposal = None
 
     def __enter__(self):
         return self
