@@ -175,7 +175,7 @@ def main() -> int:
     ap.add_argument("--impl", default="tfim", choices=["tfim", "reference"])
     ap.add_argument("--workload", default="cfg4", choices=sorted(WORKLOADS))
     ap.add_argument("--counter", default="auto", choices=["auto", "lop3", "tensor"])
-    ap.add_argument("--lookahead", type=int, default=1)
+    ap.add_argument("--lookahead", default="learned", choices=["off", "filtered", "learned", "all"])
     ap.add_argument("--ref-scale", type=float, default=0.02)
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-plain", action="store_true")
@@ -219,7 +219,7 @@ def main() -> int:
 
     db = tf.Database.from_csr(off_np, items_np, w["minsup"], device=local)
     info = db.info
-    mine_kw = dict(engine="batched", counter=args.counter, lookahead=bool(args.lookahead))
+    mine_kw = dict(engine="batched", counter=args.counter, lookahead=args.lookahead)
     for _ in range(args.warmup):
         db.mine(**mine_kw)
     barrier()
@@ -308,7 +308,7 @@ def main() -> int:
                    "reduced_rows": info["trans_num_reduced"], "survivors": info["n_survivors"],
                    "bitmap_bytes": int(info["n_dense"]) * int(info["words_per_row"]) * 4,
                    "l2": "inputs larger than L2 (bitmap) and a 256 MB L2 flush before every timed step",
-                   "engine": "batched", "counter": args.counter, "lookahead": bool(args.lookahead),
+                   "engine": "batched", "counter": args.counter, "lookahead": args.lookahead,
                    "parallelism": f"{world} independent database replicas, one per GPU"},
         "mine_time_s": ms / 1000.0,
         "plain_mine_time_s": plain.stats["device_ms"] / 1000.0 if plain else None,
