@@ -150,7 +150,9 @@ TFIM_API int tfim_count_wave_noalloc(const uint32_t* d_bitmap, int64_t words_per
 
 /* mining engines */
 #define TFIM_ENGINE_PLAIN    0   /* the reference's search, one counted node per launch */
-#define TFIM_ENGINE_BATCHED  1   /* pruned search counted in waves of families */
+#define TFIM_ENGINE_BATCHED  1   /* pruned search counted in waves of families (host-driven) */
+#define TFIM_ENGINE_RESIDENT 2   /* the same search with its state on the device: pack and
+                                    expand kernels, one status read per wave */
 
 typedef struct {
     int32_t engine;        /* TFIM_ENGINE_* */

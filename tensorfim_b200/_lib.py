@@ -23,6 +23,7 @@ TFIM_E_IO = 7
 
 ENGINE_PLAIN = 0
 ENGINE_BATCHED = 1
+ENGINE_RESIDENT = 2
 COUNTER_AUTO = 0
 COUNTER_LOP3 = 1
 COUNTER_TENSOR = 2

@@ -58,6 +58,7 @@ int count_wave_impl(tfim_ctx* c, int32_t b, int32_t min_count, const int32_t* d_
     std::vector<JobDesc> jobs(1);
     jobs[0].base_slot = -1; jobs[0].base_item = -1;
     jobs[0].n_rows = b; jobs[0].n_cols = d; jobs[0].row_off = 0; jobs[0].col_off = 0; jobs[0].out_off = 0;
+    jobs[0].self_col = -1; jobs[0].pad = 0;
     std::vector<RowDesc> rows(b);
     for (int32_t i = 0; i < b; i++) rows[i] = RowDesc{i, -1};
     std::vector<int32_t> cols(d);
@@ -273,6 +274,7 @@ int tfim_mine(tfim_ctx* c, const tfim_mine_opts* opts, tfim_mine_stats* stats) {
     int rc;
     if (o.engine == TFIM_ENGINE_PLAIN) rc = mine_plain(c, &o, &st);
     else if (o.engine == TFIM_ENGINE_BATCHED) rc = mine_batched(c, &o, &st);
+    else if (o.engine == TFIM_ENGINE_RESIDENT) rc = mine_resident(c, &o, &st);
     else { set_error("unknown engine %d", o.engine); return TFIM_E_INVALID; }
     cudaEventRecord(e_end, c->stream);
     cudaEventSynchronize(e_end);
@@ -411,6 +413,8 @@ void tfim_close(tfim_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->engine) tfim::free_engine(c->engine);
     c->engine = nullptr;
+    if (c->resident) tfim::free_resident(c->resident, c->stream);
+    c->resident = nullptr;
     tfim::dev_free(c->d_bitmap, c->stream);
     tfim::dev_free(c->d_red_off, c->stream);
     tfim::dev_free(c->d_red_items, c->stream);

@@ -81,7 +81,7 @@ __global__ void __launch_bounds__(256) k_count_b1(CountArgs a) {
     } else if (tid < 128) {
         const int c = tid - 64;
         if (t.c0 + c < t.c1) {
-            const int32_t col = a.cols[j.col_off + t.c0 + c];
+            const int32_t col = (t.c0 + c) == j.self_col ? -1 : a.cols[j.col_off + t.c0 + c];
             if (col >= 0) { col_src[c] = a.bitmap + (int64_t)col * W; col_kind[c] = 0; }
             else { col_src[c] = nullptr; col_kind[c] = 1; }
         } else {

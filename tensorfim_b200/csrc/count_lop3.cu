@@ -51,7 +51,7 @@ __global__ void __launch_bounds__(256) k_count_lop3(CountArgs a) {
         __syncthreads();
         // 2. one warp per column: stream the column row through every staged row
         for (int c = t.c0 + warp; c < t.c1; c += 8) {
-            const int32_t col = a.cols[j.col_off + c];
+            const int32_t col = c == j.self_col ? -1 : a.cols[j.col_off + c];
             const uint4* cp = col >= 0 ? reinterpret_cast<const uint4*>(a.bitmap + (int64_t)col * W) + w4b : nullptr;
             uint32_t acc[kLop3Rows];
 #pragma unroll

@@ -87,11 +87,13 @@ struct SlotPool {
     void flush() { free_list.insert(free_list.end(), deferred.begin(), deferred.end()); deferred.clear(); }
 };
 
+}  // namespace
+
 // Tile builders --------------------------------------------------------------------------
 // `upper`: the job's rows and columns are the same list; only tiles holding some (i, j>=i)
 // are emitted and the mirror pass fills the rest.
 void tiles_lop3(int32_t job, int32_t nr, int32_t nc, int64_t W, int64_t wslice, std::vector<TileDesc>& out,
-                bool upper = false) {
+                bool upper) {
     for (int32_t r0 = 0; r0 < nr; r0 += kLop3Rows)
         for (int32_t c0 = 0; c0 < nc; c0 += 64)
             for (int64_t w0 = 0; w0 < W; w0 += wslice) {
@@ -105,7 +107,7 @@ void tiles_lop3(int32_t job, int32_t nr, int32_t nc, int64_t W, int64_t wslice, 
             }
 }
 void tiles_b1(int32_t job, int32_t nr, int32_t nc, int64_t W, int64_t kslice, std::vector<TileDesc>& out,
-              bool upper = false) {
+              bool upper) {
     for (int64_t w0 = 0; w0 < W; w0 += kslice)
         for (int32_t r0 = 0; r0 < nr; r0 += kB1Rows)
             for (int32_t c0 = 0; c0 < nc; c0 += kB1Cols) {
@@ -118,6 +120,8 @@ void tiles_b1(int32_t job, int32_t nr, int32_t nc, int64_t W, int64_t kslice, st
                 out.push_back(t);
             }
 }
+
+namespace {
 
 // A wave of count jobs, ready to upload.
 struct Wave {
@@ -147,6 +151,8 @@ struct Wave {
         j.n_rows = (int32_t)rs.size(); j.n_cols = (int32_t)cs.size();
         j.row_off = (int32_t)rows.size(); j.col_off = (int32_t)cols.size();
         j.out_off = out_total;
+        j.self_col = -1;
+        j.pad = 0;
         const int32_t id = (int32_t)jobs.size();
         jobs.push_back(j);
         use_b1.push_back(b1);
@@ -481,6 +487,19 @@ int mine_plain(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* st) {
     WaveRunner& wr = es.wr;
     wr.counter = TFIM_COUNTER_LOP3;
     int rc = run_plain(c, c->roots, wr, es.pool, st);
+    st->launches += wr.launches;
+    st->count_launches += wr.count_launches;
+    st->bytes_alg += wr.bytes_alg;
+    st->kernel_ms += wr.kernel_ms;
+    st->sync_ms += wr.sync_ms;
+    return rc;
+}
+
+int mine_plain_roots(tfim_ctx* c, const std::vector<int32_t>& roots, tfim_mine_stats* st) {
+    EngineState& es = engine_state(c);
+    WaveRunner& wr = es.wr;
+    wr.counter = TFIM_COUNTER_LOP3;
+    int rc = run_plain(c, roots, wr, es.pool, st);
     st->launches += wr.launches;
     st->count_launches += wr.count_launches;
     st->bytes_alg += wr.bytes_alg;

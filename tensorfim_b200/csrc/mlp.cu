@@ -208,6 +208,14 @@ int mlp_grad_device(Mlp* m, const float* d_x, const float* d_y, int64_t n, float
     return TFIM_OK;
 }
 
+int mlp_device_params(tfim_mlp* h, const void** wbf, const float** params) {
+    Mlp* m = (Mlp*)h;
+    TFIM_CHECK(m, TFIM_E_INVALID, "null network");
+    *wbf = m->d_wbf;
+    *params = m->d_params;
+    return TFIM_OK;
+}
+
 }  // namespace tfim
 
 using namespace tfim;

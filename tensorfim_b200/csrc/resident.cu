@@ -1,0 +1,1220 @@
+// RESIDENT engine: the batched search with its state on the device.
+//
+// Same search and pruning as mine_batched (mine.cu) -- families of children counted as
+// masked Gram blocks, candidate restriction, equal-support pruning, head-union-tail
+// lookahead with the tail-pair filter or the learned proposal, dynamic tail order, root
+// filter -- but the family records, the DFS stack, the lookahead queue, the mask-slot
+// free list and the MFI output live in device memory, and two kernels drive it:
+//   k_res_pack    (one block) pops families from the top of the device stack into a wave:
+//                 count-job descriptors, counted rows, tiles and output offsets;
+//   k_res_expand  (one warp per counted row) turns a counted row into the child's MFI
+//                 test, equal-support pruning, tail (sorted by support in the warp),
+//                 child mask, lookahead decision (tail-pair filter, or the proposal MLP
+//                 evaluated in the warp) and pushes the child onto the stack.
+// Between them the counting kernels of count_lop3.cu / count_b1.cu run on the wave.  The
+// host reads one small status record per wave (to size the launches and grow pools) and
+// copies the MFIs back once at the end.
+#include <cub/cub.cuh>
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+#include "tfim_internal.h"
+
+namespace tfim {
+namespace {
+
+struct DFam {
+    int32_t slot, item;        // base mask = masks[slot] & B[item] (either optional)
+    int32_t head_off, head_len;
+    int32_t F_off, nF, nT;     // F list in the item pool, tail = its first nT entries
+    int32_t sup;
+    int32_t next_row;          // rows handed to waves
+    int32_t rows_done;         // rows expanded
+    int32_t state;             // 0 ready, 1 waiting on its lookahead, 2 finished
+    int32_t top;               // 1: the family of the empty prefix
+};
+
+struct DLook {
+    int32_t fam, slot, log, pad;
+};
+
+enum { kJobFam = 0, kJobLook = 1 };
+struct DJob {
+    int32_t fam, kind, r0, nr, slot, log;
+    int32_t b3, b1;            // exclusive prefix of base CUDA-core / tensor-core tiles over the wave's jobs
+};
+
+struct ResStatus {
+    int32_t stack_n, look_n, fam_n, item_n, head_n, mfi_n, mfi_item_n, slot_n, free_n, free_taken, defer_n, log_n;
+    int32_t jobs, rows, tiles_l3, tiles_b1;
+    int64_t out_total;
+    int32_t max_cols, max_head, starved, error;
+    unsigned long long supports, nodes, lookaheads, hits, skipped, pep;
+};
+
+struct ResPtrs {
+    // pools
+    DFam* fams;
+    int32_t* items;
+    int32_t* heads;
+    int32_t* stack;
+    DLook* looks;
+    int32_t* free_slots;
+    int32_t* defer;
+    int32_t* mfi_off;
+    int32_t* mfi_len;
+    int32_t* mfi_sup;
+    int32_t* mfi_items;
+    float* log_feat;
+    float* log_label;
+    // wave
+    DJob* djobs;
+    JobDesc* jobs;
+    RowDesc* rows;
+    int32_t* row_job;
+    int32_t* row_local;
+    TileDesc* tiles_l3;
+    TileDesc* tiles_b1;
+    int32_t* counts;
+    // constants
+    const uint32_t* bitmap;
+    uint32_t* masks;
+    const int32_t* dense_freq;
+    const uint8_t* is_root;
+    const __nv_bfloat16* mlp_w;   // BF16 weights of the proposal (nullptr: none)
+    const float* mlp_p;           // FP32 parameters (biases read from here)
+    ResStatus* st;
+    int64_t W, n_bits;
+    int32_t min_count;
+    int32_t wave_rows;            // cap on rows per wave
+    int64_t cap_out, cap_tiles;
+    int32_t counter;              // TFIM_COUNTER_*
+    int32_t la_mode;              // 0 off, 1 filtered, 2 learned, 3 every node
+    int32_t log_on;
+    float proposal_threshold;
+    int64_t kslice_min;           // b1 word slice when tiles are few (multiple of 64)
+    int32_t sm_count;
+};
+
+__host__ __device__ __forceinline__ int64_t lmin(int64_t a, int64_t b) { return a < b ? a : b; }
+__host__ __device__ __forceinline__ int64_t lmax(int64_t a, int64_t b) { return a > b ? a : b; }
+
+constexpr int kPackThreads = 1024;
+constexpr int kPackItems = 4;
+constexpr int kPackCand = kPackThreads * kPackItems;
+
+__device__ __forceinline__ bool use_b1_shape(const ResPtrs& p, int nr, int nc) {
+    if (p.counter == TFIM_COUNTER_LOP3) return false;
+    if (p.counter == TFIM_COUNTER_TENSOR) return true;
+    return nr >= 16 && nc >= 16;
+}
+__device__ __forceinline__ int64_t l3_tiles(int nr, int nc) { return (int64_t)((nr + kLop3Rows - 1) / kLop3Rows) * ((nc + 63) / 64); }
+__device__ __forceinline__ int64_t b1_tiles(int nr, int nc) { return (int64_t)((nr + kB1Rows - 1) / kB1Rows) * ((nc + kB1Cols - 1) / kB1Cols); }
+
+// ---------------------------------------------------------------------------------- pack
+// One block.  Phases: (0) recycle the mask slots released by the last expand; (1) one job
+// per queued lookahead; (2) families from the top of the stack, 4096 candidates per pass,
+// with block scans deciding how many fit the wave's row and output budgets; (3) the counted
+// rows and row->job maps; (4) tiles (split-k slices chosen from the wave's base tile count).
+// Every phase is block-parallel; jobs are ordered by their row offsets, which the row and
+// tile writers binary-search.
+__device__ __forceinline__ int find_job_by_row(const JobDesc* jobs, int nj, int32_t g) {
+    int lo = 0, hi = nj - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (jobs[mid].row_off <= g) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+template <bool B1>
+__device__ __forceinline__ int find_job_by_tile(const DJob* dj, int nj, int64_t t) {
+    int lo = 0, hi = nj - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if ((B1 ? dj[mid].b1 : dj[mid].b3) <= t) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(kPackThreads) k_res_pack(ResPtrs p) {
+    typedef cub::BlockScan<int64_t, kPackThreads> Scan;
+    typedef cub::BlockReduce<int64_t, kPackThreads> Red;
+    __shared__ union {
+        typename Scan::TempStorage scan;
+        typename Red::TempStorage red;
+    } tmp;
+    __shared__ int32_t s_fam[kPackCand];
+    __shared__ int32_t s_n_jobs, s_rows_total, s_done, s_max_cols, s_max_head, s_stack_after, s_kstop;
+    __shared__ int64_t s_out_total, s_agg;
+    ResStatus* st = p.st;
+    const int tid = threadIdx.x;
+    // (0) recycle
+    const int32_t taken = min(st->free_taken, st->free_n);
+    const int32_t fn = st->free_n - taken, dn = st->defer_n;
+    for (int k = tid; k < dn; k += kPackThreads) p.free_slots[fn + k] = p.defer[k];
+    if (tid == 0) {
+        s_n_jobs = 0; s_rows_total = 0; s_out_total = 0; s_max_cols = 0; s_max_head = 0; s_done = 0;
+        s_stack_after = st->stack_n;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        st->free_n = fn + dn;
+        st->free_taken = 0;
+        st->defer_n = 0;
+    }
+    // (1) lookahead jobs
+    const int32_t n_look = st->look_n;
+    for (int base = 0; base < n_look; base += kPackCand) {
+        int64_t v[kPackItems], ex[kPackItems];
+        int64_t mc = 0;
+        for (int q = 0; q < kPackItems; q++) {
+            const int k = base + tid * kPackItems + q;
+            v[q] = 0;
+            if (k < n_look) {
+                const DFam f = p.fams[p.looks[k].fam];
+                v[q] = f.nF - f.nT + 1;
+                mc = max(mc, v[q]);
+            }
+        }
+        Scan(tmp.scan).ExclusiveSum(v, ex, s_agg);
+        __syncthreads();
+        const int64_t agg = s_agg;
+        const int64_t mcb = Red(tmp.red).Reduce(mc, cub::Max());
+        for (int q = 0; q < kPackItems; q++) {
+            const int k = base + tid * kPackItems + q;
+            if (k >= n_look) continue;
+            const DLook L = p.looks[k];
+            const DFam f = p.fams[L.fam];
+            DJob dj;
+            dj.fam = L.fam; dj.kind = kJobLook; dj.r0 = 0; dj.nr = 1; dj.slot = L.slot; dj.log = L.log; dj.b3 = 0; dj.b1 = 0;
+            p.djobs[k] = dj;
+            JobDesc jd;
+            jd.base_slot = -1; jd.base_item = -1; jd.n_rows = 1; jd.n_cols = f.nF - f.nT + 1;
+            jd.row_off = k; jd.col_off = f.F_off + f.nT; jd.out_off = s_out_total + ex[q]; jd.self_col = f.nF - f.nT; jd.pad = 0;
+            p.jobs[k] = jd;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            s_out_total += agg;
+            s_max_cols = max(s_max_cols, (int32_t)mcb);
+        }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        s_rows_total = n_look;
+        s_n_jobs = n_look;
+        st->look_n = 0;
+    }
+    __syncthreads();
+    // (2) families from the top of the stack
+    while (!s_done) {
+        const int32_t avail = s_stack_after;
+        const int32_t n_c = min(avail, kPackCand);
+        if (n_c == 0) break;
+        const int64_t rows_left = (int64_t)p.wave_rows - s_rows_total;
+        const int64_t out_left = p.cap_out - s_out_total;
+        const bool wave_empty = s_n_jobs == 0;
+        int64_t rv[kPackItems], ov[kPackItems], rc[kPackItems], oc[kPackItems];
+        int32_t nf[kPackItems], hl[kPackItems];
+        for (int q = 0; q < kPackItems; q++) {
+            const int k = tid * kPackItems + q;
+            rv[q] = ov[q] = 0;
+            nf[q] = 0;
+            hl[q] = 0;
+            if (k < n_c) {
+                const int32_t fid = p.stack[avail - 1 - k];
+                const DFam f = p.fams[fid];
+                s_fam[k] = fid;
+                const int32_t rem = f.state == 0 ? f.nT - f.next_row : 0;
+                rv[q] = rem;
+                ov[q] = (int64_t)rem * f.nF;
+                nf[q] = f.nF;
+                hl[q] = f.head_len;
+            }
+        }
+        Scan(tmp.scan).InclusiveSum(rv, rc);
+        __syncthreads();
+        Scan(tmp.scan).InclusiveSum(ov, oc);
+        __syncthreads();
+        // take per candidate and the first stop point
+        int32_t take[kPackItems];
+        int64_t kstop_local = n_c;
+        for (int q = 0; q < kPackItems; q++) {
+            const int k = tid * kPackItems + q;
+            take[q] = -1;
+            if (k >= n_c) continue;
+            const int64_t r_before = rc[q] - rv[q], o_before = oc[q] - ov[q];
+            if (rc[q] <= rows_left && oc[q] <= out_left) {
+                take[q] = (int32_t)rv[q];
+            } else if (r_before < rows_left && o_before < out_left) {
+                int64_t t_rows = min(rows_left - r_before, (out_left - o_before) / max(1, nf[q]));
+                take[q] = (int32_t)min(t_rows, rv[q]);
+                if (take[q] == 0 && r_before == 0 && o_before == 0 && wave_empty) atomicExch(&st->starved, 1);
+            }
+            const bool stop = take[q] < 0 || (rv[q] > 0 && take[q] < rv[q]);
+            if (stop) kstop_local = min(kstop_local, (int64_t)k);
+        }
+        const int64_t kstop = Red(tmp.red).Reduce(kstop_local, cub::Min());
+        if (tid == 0) s_kstop = (int32_t)kstop;
+        __syncthreads();
+        const int32_t ks = s_kstop;
+        // jobs: candidates before the stop point with rows left, and the stop point if it takes rows
+        int64_t hj[kPackItems], hx[kPackItems], tr[kPackItems];
+        int64_t mcol = 0, mhead = 0;
+        for (int q = 0; q < kPackItems; q++) {
+            const int k = tid * kPackItems + q;
+            hj[q] = 0;
+            tr[q] = 0;
+            if (k < n_c && ((k < ks && rv[q] > 0) || (k == ks && take[q] > 0))) {
+                hj[q] = 1;
+                tr[q] = take[q];
+                mcol = max(mcol, (int64_t)nf[q]);
+                mhead = max(mhead, (int64_t)hl[q]);
+            }
+        }
+        Scan(tmp.scan).ExclusiveSum(hj, hx, s_agg);
+        __syncthreads();
+        const int64_t n_new = s_agg;
+        int64_t trx[kPackItems];
+        Scan(tmp.scan).ExclusiveSum(tr, trx, s_agg);
+        __syncthreads();
+        const int64_t rows_new = s_agg;
+        const int64_t mcb = Red(tmp.red).Reduce(mcol, cub::Max());
+        __syncthreads();
+        const int64_t mhb = Red(tmp.red).Reduce(mhead, cub::Max());
+        for (int q = 0; q < kPackItems; q++) {
+            const int k = tid * kPackItems + q;
+            if (!hj[q]) continue;
+            const int32_t fid = s_fam[k];
+            DFam* fp = p.fams + fid;
+            const DFam f = *fp;
+            const int32_t jid = s_n_jobs + (int32_t)hx[q];
+            DJob dj;
+            dj.fam = fid; dj.kind = kJobFam; dj.r0 = f.next_row; dj.nr = take[q]; dj.slot = -1; dj.log = -1; dj.b3 = 0; dj.b1 = 0;
+            p.djobs[jid] = dj;
+            JobDesc jd;
+            jd.base_slot = f.slot; jd.base_item = f.item; jd.n_rows = take[q]; jd.n_cols = f.nF;
+            jd.row_off = s_rows_total + (int32_t)trx[q];
+            jd.col_off = f.F_off;
+            // outputs: every candidate before this one contributed rv * nF, this one take * nF
+            jd.out_off = s_out_total + (oc[q] - ov[q]);
+            jd.self_col = -1; jd.pad = 0;
+            p.jobs[jid] = jd;
+            fp->next_row = f.next_row + take[q];
+        }
+        __syncthreads();
+        // outputs of this pass: every job's taken rows x its columns
+        int64_t contrib = 0;
+        for (int q = 0; q < kPackItems; q++) contrib += (int64_t)(hj[q] ? (int64_t)tr[q] * nf[q] : 0);
+        const int64_t out_pass = Red(tmp.red).Sum(contrib);
+        if (tid == 0) {
+            s_n_jobs += (int32_t)n_new;
+            s_rows_total += (int32_t)rows_new;
+            s_out_total += out_pass;
+            s_max_cols = max(s_max_cols, (int32_t)mcb);
+            s_max_head = max(s_max_head, (int32_t)mhb);
+            s_stack_after -= ks;   // candidates before the stop point are consumed
+            if (ks < n_c || s_rows_total >= p.wave_rows || n_c < kPackCand || s_stack_after == 0) s_done = 1;
+        }
+        __syncthreads();
+    }
+    __syncthreads();
+    const int32_t nj = s_n_jobs, rows_total = s_rows_total;
+    // (3) rows
+    for (int32_t g = tid; g < rows_total; g += kPackThreads) {
+        const int j = find_job_by_row(p.jobs, nj, g);
+        const JobDesc jd = p.jobs[j];
+        const DJob dj = p.djobs[j];
+        const int32_t r = g - jd.row_off;
+        if (dj.kind == kJobFam) p.rows[g] = RowDesc{-1, p.items[jd.col_off + dj.r0 + r]};
+        else p.rows[g] = RowDesc{dj.slot, -1};
+        p.row_job[g] = j;
+        p.row_local[g] = r;
+    }
+    // (4) tiles: base tiles per job, prefix over jobs (chunks of kPackCand)
+    int64_t tot3 = 0, tot1 = 0;
+    for (int base = 0; base < nj; base += kPackCand) {
+        int64_t a3[kPackItems], a1[kPackItems], x3[kPackItems], x1[kPackItems];
+        for (int q = 0; q < kPackItems; q++) {
+            const int j = base + tid * kPackItems + q;
+            a3[q] = a1[q] = 0;
+            if (j < nj) {
+                const JobDesc jd = p.jobs[j];
+                const bool b1 = use_b1_shape(p, jd.n_rows, jd.n_cols) && p.djobs[j].kind == kJobFam;
+                if (b1) a1[q] = b1_tiles(jd.n_rows, jd.n_cols);
+                else a3[q] = l3_tiles(jd.n_rows, jd.n_cols);
+            }
+        }
+        Scan(tmp.scan).ExclusiveSum(a3, x3, s_agg);
+        __syncthreads();
+        const int64_t g3 = s_agg;
+        Scan(tmp.scan).ExclusiveSum(a1, x1, s_agg);
+        __syncthreads();
+        const int64_t g1 = s_agg;
+        for (int q = 0; q < kPackItems; q++) {
+            const int j = base + tid * kPackItems + q;
+            if (j >= nj) continue;
+            // b3/b1 hold the prefix; a job's own count is recomputed from its shape
+            p.djobs[j].b3 = (int32_t)(tot3 + x3[q]);
+            p.djobs[j].b1 = (int32_t)(tot1 + x1[q]);
+        }
+        tot3 += g3;
+        tot1 += g1;
+        __syncthreads();
+    }
+    const int64_t W = p.W;
+    int64_t ks1 = tot1 > 0 ? lmax(1, (4LL * p.sm_count + tot1 - 1) / tot1) : 1;
+    ks1 = lmin(ks1, lmax(1, W / 64));
+    int64_t kslice = ((W / 64 + ks1 - 1) / ks1) * 64;
+    int64_t ws3 = tot3 > 0 ? lmax(1, (8LL * p.sm_count + tot3 - 1) / tot3) : 1;
+    ws3 = lmin(ws3, lmax(1, W / 256));
+    int64_t wslice = ((W / 64 + ws3 - 1) / ws3) * 64;
+    if (kslice <= 0) kslice = 64;
+    if (wslice <= 0) wslice = 64;
+    const int64_t nk = W > 0 ? (W + kslice - 1) / kslice : 1, nw = W > 0 ? (W + wslice - 1) / wslice : 1;
+    const int64_t T3 = tot3 * nw, T1 = tot1 * nk;
+    __syncthreads();
+    if (T3 <= p.cap_tiles)
+        for (int64_t t = tid; t < T3; t += kPackThreads) {
+            const int64_t slice = t / tot3, local = t % tot3;
+            const int j = find_job_by_tile<false>(p.djobs, nj, local);
+            const JobDesc jd = p.jobs[j];
+            const int64_t within = local - p.djobs[j].b3;
+            const int cg = (jd.n_cols + 63) / 64;
+            const int rg = (int)(within / cg), cc = (int)(within % cg);
+            const int64_t w0 = slice * wslice;
+            p.tiles_l3[t] = TileDesc{j, rg * kLop3Rows, min(kLop3Rows, jd.n_rows - rg * kLop3Rows), cc * 64,
+                                     min(jd.n_cols, cc * 64 + 64), (int32_t)w0, (int32_t)lmin(W, w0 + wslice), 0};
+        }
+    if (T1 <= p.cap_tiles)
+        for (int64_t t = tid; t < T1; t += kPackThreads) {
+            const int64_t slice = t / tot1, local = t % tot1;
+            const int j = find_job_by_tile<true>(p.djobs, nj, local);
+            const JobDesc jd = p.jobs[j];
+            const int64_t within = local - p.djobs[j].b1;
+            const int cg = (jd.n_cols + kB1Cols - 1) / kB1Cols;
+            const int rg = (int)(within / cg), cc = (int)(within % cg);
+            const int64_t w0 = slice * kslice;
+            p.tiles_b1[t] = TileDesc{j, rg * kB1Rows, min(kB1Rows, jd.n_rows - rg * kB1Rows), cc * kB1Cols,
+                                     min(jd.n_cols, cc * kB1Cols + kB1Cols), (int32_t)w0, (int32_t)lmin(W, w0 + kslice), 0};
+        }
+    if (tid == 0) {
+        if (T1 > p.cap_tiles || T3 > p.cap_tiles) st->error = 2;   // tile capacity exceeded
+        st->jobs = nj;
+        st->rows = rows_total;
+        st->tiles_l3 = (int32_t)T3;
+        st->tiles_b1 = (int32_t)T1;
+        st->out_total = s_out_total;
+        st->max_cols = s_max_cols;
+        st->max_head = s_max_head;
+        st->stack_n = s_stack_after;
+        st->nodes += rows_total;
+        st->supports += s_out_total;
+    }
+}
+
+// ---------------------------------------------------------------------------------- expand helpers
+__device__ __forceinline__ int32_t pop_slot(const ResPtrs& p) {
+    const int32_t k = atomicAdd(&p.st->free_taken, 1);
+    const int32_t fn = p.st->free_n;
+    if (k < fn) return p.free_slots[fn - 1 - k];
+    return atomicAdd(&p.st->slot_n, 1);
+}
+__device__ __forceinline__ void release_slot(const ResPtrs& p, int32_t s) {
+    if (s < 0) return;
+    const int32_t k = atomicAdd(&p.st->defer_n, 1);
+    p.defer[k] = s;
+}
+
+// warp: dst mask row = (slot>=0 ? masks[slot] : ~0) & (item>=0 ? B[item] : ~0) & AND of list
+__device__ void warp_build_mask(const ResPtrs& p, int32_t dst, int32_t slot, int32_t item, int32_t t, const int32_t* extra,
+                                int n_extra, int lane) {
+    const int64_t W4 = p.W >> 2;
+    uint4* d = reinterpret_cast<uint4*>(p.masks + (int64_t)dst * p.W);
+    const uint4* sm = slot >= 0 ? reinterpret_cast<const uint4*>(p.masks + (int64_t)slot * p.W) : nullptr;
+    const uint4* si = item >= 0 ? reinterpret_cast<const uint4*>(p.bitmap + (int64_t)item * p.W) : nullptr;
+    const uint4* st = t >= 0 ? reinterpret_cast<const uint4*>(p.bitmap + (int64_t)t * p.W) : nullptr;
+    for (int64_t w = lane; w < W4; w += 32) {
+        uint4 v = make_uint4(~0u, ~0u, ~0u, ~0u);
+        auto andv = [&](uint4 x) { v.x &= x.x; v.y &= x.y; v.z &= x.z; v.w &= x.w; };
+        if (sm) andv(sm[w]);
+        if (si) andv(__ldg(si + w));
+        if (st) andv(__ldg(st + w));
+        for (int q = 0; q < n_extra; q++) andv(__ldg(reinterpret_cast<const uint4*>(p.bitmap + (int64_t)extra[q] * p.W) + w));
+        d[w] = v;
+    }
+}
+
+__device__ void warp_emit_mfi(const ResPtrs& p, const int32_t* head, int head_len, int32_t t, const int32_t* extra_cols,
+                              int n_extra, const int32_t* F, int32_t sup, int lane) {
+    // max dense id decides the root rule
+    int32_t mx = t;
+    for (int q = lane; q < head_len; q += 32) mx = max(mx, head[q]);
+    for (int q = lane; q < n_extra; q += 32) mx = max(mx, F[extra_cols[q]]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if (!p.is_root[mx]) return;
+    const int len = head_len + 1 + n_extra;
+    int32_t k = 0, off = 0;
+    if (lane == 0) {
+        k = atomicAdd(&p.st->mfi_n, 1);
+        off = atomicAdd(&p.st->mfi_item_n, len);
+    }
+    k = __shfl_sync(0xffffffffu, k, 0);
+    off = __shfl_sync(0xffffffffu, off, 0);
+    for (int q = lane; q < head_len; q += 32) p.mfi_items[off + q] = head[q];
+    if (lane == 0) p.mfi_items[off + head_len] = t;
+    for (int q = lane; q < n_extra; q += 32) p.mfi_items[off + head_len + 1 + q] = F[extra_cols[q]];
+    if (lane == 0) {
+        p.mfi_off[k] = off;
+        p.mfi_len[k] = len;
+        p.mfi_sup[k] = len == 1 ? p.dense_freq[t] : sup;   // a root's own frequency is its F1 count
+    }
+}
+
+__device__ void finish_row(const ResPtrs& p, DFam* f, int lane) {
+    if (lane == 0) {
+        const int32_t done = atomicAdd(&f->rows_done, 1) + 1;
+        if (done == f->nT) {
+            release_slot(p, f->slot);
+            f->state = 2;
+        }
+    }
+}
+
+// The proposal network on one warp: lane i holds feature i.
+__device__ float warp_mlp(const ResPtrs& p, float x, int lane) {
+    const __nv_bfloat16* w = p.mlp_w;
+    const float* P = p.mlp_p;
+    constexpr int kIn = 32, kH = 64;
+    constexpr int oW1 = 0, oB1 = kH * kIn, oW2 = oB1 + kH, oB2 = oW2 + kH * kH, oW3 = oB2 + kH, oB3 = oW3 + kH;
+    float h1a = P[oB1 + lane], h1b = P[oB1 + lane + 32];
+    for (int i = 0; i < kIn; i++) {
+        const float xi = __shfl_sync(0xffffffffu, x, i);
+        h1a = fmaf(__bfloat162float(w[oW1 + lane * kIn + i]), xi, h1a);
+        h1b = fmaf(__bfloat162float(w[oW1 + (lane + 32) * kIn + i]), xi, h1b);
+    }
+    h1a = fmaxf(h1a, 0.f);
+    h1b = fmaxf(h1b, 0.f);
+    float h2a = P[oB2 + lane], h2b = P[oB2 + lane + 32];
+    for (int j = 0; j < kH; j++) {
+        const float hj = __shfl_sync(0xffffffffu, j < 32 ? h1a : h1b, j & 31);
+        h2a = fmaf(__bfloat162float(w[oW2 + lane * kH + j]), hj, h2a);
+        h2b = fmaf(__bfloat162float(w[oW2 + (lane + 32) * kH + j]), hj, h2b);
+    }
+    float z = __bfloat162float(w[oW3 + lane]) * fmaxf(h2a, 0.f) + __bfloat162float(w[oW3 + lane + 32]) * fmaxf(h2b, 0.f);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) z += __shfl_xor_sync(0xffffffffu, z, o);
+    z += P[oB3];
+    return 1.f / (1.f + expf(-z));
+}
+
+// ---------------------------------------------------------------------------------- expand
+// One warp per counted row of the wave.
+__global__ void __launch_bounds__(256) k_res_expand(ResPtrs p) {
+    const int64_t g = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    ResStatus* st = p.st;
+    if (g >= st->rows) return;
+    const int32_t jid = p.row_job[g];
+    const int32_t r = p.row_local[g];
+    const DJob dj = p.djobs[jid];
+    const JobDesc jd = p.jobs[jid];
+    const int32_t* crow = p.counts + jd.out_off + (int64_t)r * jd.n_cols;
+    const int32_t minc = p.min_count;
+    DFam* fp = p.fams + dj.fam;
+    const DFam f = *fp;
+    const int32_t* F = p.items + f.F_off;
+
+    if (dj.kind == kJobLook) {
+        const int32_t self = crow[jd.n_cols - 1];
+        bool ext = false;
+        for (int c = lane; c < jd.n_cols - 1; c += 32) ext |= crow[c] >= minc;
+        ext = __any_sync(0xffffffffu, ext);
+        if (lane == 0) {
+            release_slot(p, dj.slot);
+            if (dj.log >= 0) p.log_label[dj.log] = self >= minc ? 1.f : 0.f;
+        }
+        if (self >= minc) {
+            if (lane == 0) atomicAdd(&st->hits, 1ull);
+            if (!ext) {
+                // head + whole tail: the tail is F[0..nT)
+                const int32_t* head = p.heads + f.head_off;
+                // emit head + F[0] ... F[nT-1]: treat F[0] as "t" and the rest as extra columns
+                int32_t mx = -1;
+                for (int q = lane; q < f.head_len; q += 32) mx = max(mx, head[q]);
+                for (int q = lane; q < f.nT; q += 32) mx = max(mx, F[q]);
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+                if (mx >= 0 && p.is_root[mx]) {
+                    const int len = f.head_len + f.nT;
+                    int32_t k = 0, off = 0;
+                    if (lane == 0) {
+                        k = atomicAdd(&st->mfi_n, 1);
+                        off = atomicAdd(&st->mfi_item_n, len);
+                    }
+                    k = __shfl_sync(0xffffffffu, k, 0);
+                    off = __shfl_sync(0xffffffffu, off, 0);
+                    for (int q = lane; q < f.head_len; q += 32) p.mfi_items[off + q] = head[q];
+                    for (int q = lane; q < f.nT; q += 32) p.mfi_items[off + f.head_len + q] = F[q];
+                    if (lane == 0) {
+                        p.mfi_off[k] = off;
+                        p.mfi_len[k] = len;
+                        p.mfi_sup[k] = len == 1 ? p.dense_freq[F[0]] : self;
+                    }
+                }
+            }
+            if (lane == 0) {
+                release_slot(p, f.slot);
+                fp->state = 2;
+            }
+        } else if (lane == 0) {
+            fp->state = 0;
+            const int32_t k = atomicAdd(&st->stack_n, 1);
+            p.stack[k] = dj.fam;
+        }
+        return;
+    }
+
+    // a family row: the child X = head(P) + t
+    const int32_t i = dj.r0 + r;
+    const int32_t nT = f.nT, nF = f.nF;
+    const int32_t t = F[i];
+    const int32_t supc = crow[i];
+    if (supc < minc) {   // cannot happen: t is in F(P)
+        if (lane == 0) atomicExch(&st->error, 1);
+        finish_row(p, fp, lane);
+        return;
+    }
+    // scan the row: extensions, equal-support items, tail
+    bool prune = false;
+    int n_ext = 0, n_eq = 0, n_tail = 0;
+    for (int c0 = 0; c0 < nF; c0 += 32) {
+        const int c = c0 + lane;
+        const int32_t v = c < nF && c != i ? crow[c] : -1;
+        const bool e = v >= minc;
+        const bool in_tail = c > i && c < nT;
+        const bool eq = e && v == supc;
+        prune |= eq && !in_tail;
+        n_ext += __popc(__ballot_sync(0xffffffffu, e));
+        n_eq += __popc(__ballot_sync(0xffffffffu, eq));
+        n_tail += __popc(__ballot_sync(0xffffffffu, e && !eq && in_tail));
+    }
+    prune = __any_sync(0xffffffffu, prune);
+    if (prune) {
+        if (lane == 0) atomicAdd(&st->pep, 1ull);
+        finish_row(p, fp, lane);
+        return;
+    }
+    const int32_t* head = p.heads + f.head_off;
+    const int n_rest = n_ext - n_eq;
+    if (n_rest == 0 || n_tail == 0) {
+        if (n_rest == 0) {
+            // MFI: head + t + the equal-support items.  Gather their columns into the item
+            // pool's scratch (the emit reads F[col]).
+            int32_t eoff = 0;
+            if (lane == 0 && n_eq) eoff = atomicAdd(&st->item_n, n_eq);
+            eoff = __shfl_sync(0xffffffffu, eoff, 0);
+            int32_t* ecols = p.items + eoff;
+            int pos = 0;
+            for (int c0 = 0; c0 < nF && n_eq; c0 += 32) {
+                const int c = c0 + lane;
+                const int32_t v = c < nF && c != i ? crow[c] : -1;
+                const bool eq = v >= minc && v == supc;
+                const unsigned bal = __ballot_sync(0xffffffffu, eq);
+                if (eq) ecols[pos + __popc(bal & ((1u << lane) - 1u))] = c;
+                pos += __popc(bal);
+            }
+            __syncwarp();
+            warp_emit_mfi(p, head, f.head_len, t, ecols, n_eq, F, supc, lane);
+        }
+        finish_row(p, fp, lane);
+        return;
+    }
+    // the child family: head' = head + t + eq; F' = sorted tail, then the other extensions
+    const int head_len = f.head_len + 1 + n_eq;
+    int32_t fid = 0, foff = 0, hoff = 0;
+    if (lane == 0) {
+        fid = atomicAdd(&st->fam_n, 1);
+        foff = atomicAdd(&st->item_n, n_rest + n_tail);   // + staging for the unsorted tail
+        hoff = atomicAdd(&st->head_n, head_len);
+    }
+    fid = __shfl_sync(0xffffffffu, fid, 0);
+    foff = __shfl_sync(0xffffffffu, foff, 0);
+    hoff = __shfl_sync(0xffffffffu, hoff, 0);
+    int32_t* Fc = p.items + foff;              // n_rest entries
+    int32_t* stage = p.items + foff + n_rest;  // n_tail tail columns in column order
+    int32_t* hc = p.heads + hoff;
+    for (int q = lane; q < f.head_len; q += 32) hc[q] = head[q];
+    if (lane == 0) hc[f.head_len] = t;
+    {
+        int pos_eq = 0, pos_tail = 0, pos_rest = 0;
+        for (int c0 = 0; c0 < nF; c0 += 32) {
+            const int c = c0 + lane;
+            const int32_t v = c < nF && c != i ? crow[c] : -1;
+            const bool e = v >= minc;
+            const bool eq = e && v == supc;
+            const bool tl = e && !eq && c > i && c < nT;
+            const bool rs = e && !eq && !tl;
+            const unsigned lt = (1u << lane) - 1u;
+            const unsigned bq = __ballot_sync(0xffffffffu, eq), bt = __ballot_sync(0xffffffffu, tl),
+                           br = __ballot_sync(0xffffffffu, rs);
+            if (eq) hc[f.head_len + 1 + pos_eq + __popc(bq & lt)] = F[c];
+            if (tl) stage[pos_tail + __popc(bt & lt)] = c;
+            if (rs) Fc[n_tail + pos_rest + __popc(br & lt)] = F[c];
+            pos_eq += __popc(bq);
+            pos_tail += __popc(bt);
+            pos_rest += __popc(br);
+        }
+    }
+    __syncwarp();
+    // tail sorted by (support, column), written as items to Fc[0 .. n_tail)
+    if (n_tail <= 32) {
+        unsigned long long key = ~0ull;
+        if (lane < n_tail) {
+            const int32_t c = stage[lane];
+            key = ((unsigned long long)(uint32_t)crow[c] << 32) | (uint32_t)c;
+        }
+        // bitonic sort across the warp, ascending
+        for (int k = 2; k <= 32; k <<= 1)
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                const unsigned long long other = __shfl_xor_sync(0xffffffffu, key, j);
+                const bool up = (lane & k) == 0;
+                const bool lower = (lane & j) == 0;
+                const bool take_min = (lower == up);
+                key = take_min ? min(key, other) : max(key, other);
+            }
+        if (lane < n_tail) Fc[lane] = F[(int32_t)(key & 0xffffffffu)];
+    } else if (n_tail <= 4096) {
+        for (int a = lane; a < n_tail; a += 32) {
+            const int32_t ca = stage[a];
+            const unsigned long long ka = ((unsigned long long)(uint32_t)crow[ca] << 32) | (uint32_t)ca;
+            int rank = 0;
+            for (int b = 0; b < n_tail; b++) {
+                const int32_t cb = stage[b];
+                const unsigned long long kb = ((unsigned long long)(uint32_t)crow[cb] << 32) | (uint32_t)cb;
+                rank += kb < ka;
+            }
+            Fc[rank] = F[ca];
+        }
+    } else {
+        for (int a = lane; a < n_tail; a += 32) Fc[a] = F[stage[a]];
+    }
+    __syncwarp();
+    // base mask of the child
+    int32_t cslot = -1, citem = -1;
+    if (f.slot < 0 && f.item < 0) {
+        citem = t;
+    } else {
+        if (lane == 0) cslot = pop_slot(p);
+        cslot = __shfl_sync(0xffffffffu, cslot, 0);
+        warp_build_mask(p, cslot, f.slot, f.item, t, nullptr, 0, lane);
+    }
+    // lookahead decision
+    bool issue = false;
+    float feat = 0.f;
+    int log_idx = -1;
+    const int list_len = n_tail + 1 + (f.item >= 0 ? 1 : 0);
+    if (p.la_mode != 0 && n_tail >= 2 && list_len <= kMaxListLen) {
+        // tail-pair filter: rows of tail items that are in this job's row range
+        int pairs = 0, pairs_ok = 0;
+        for (int a = 0; a < n_tail; a++) {
+            const int32_t ra = stage[a];
+            if (ra < dj.r0 || ra >= dj.r0 + dj.nr) continue;
+            const int32_t* rowa = p.counts + jd.out_off + (int64_t)(ra - dj.r0) * jd.n_cols;
+            for (int b = a + 1 + lane; b < n_tail; b += 32) {
+                pairs++;
+                pairs_ok += rowa[stage[b]] >= minc;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            pairs += __shfl_xor_sync(0xffffffffu, pairs, o);
+            pairs_ok += __shfl_xor_sync(0xffffffffu, pairs_ok, o);
+        }
+        const bool filtered = pairs_ok < pairs;
+        if (filtered && p.la_mode != 3) {
+            if (lane == 0) atomicAdd(&st->skipped, 1ull);
+        } else {
+            issue = true;
+            if (p.la_mode == 2 || p.log_on) {
+                // features (same definitions as the host engine's)
+                double mn = 1e30, mn2 = 1e30, mx = 0, sum = 0, sum2 = 0, logprod = 0;
+                int gt90 = 0, gt99 = 0;
+                for (int a = 0; a < n_tail; a++) {
+                    const double rr = (double)crow[stage[a]] / (double)supc;
+                    if (rr < mn) { mn2 = mn; mn = rr; } else if (rr < mn2) mn2 = rr;
+                    mx = fmax(mx, rr);
+                    sum += rr;
+                    sum2 += rr * rr;
+                    logprod += log(fmax(rr, 1e-12));
+                    gt90 += rr > 0.9;
+                    gt99 += rr > 0.99;
+                }
+                const int k = n_tail;
+                const double mean = sum / k, var = fmax(0.0, sum2 / k - mean * mean);
+                const double minc_d = max(1, minc);
+                const bool top_child = f.slot < 0 && f.item < 0;
+                const double pf = pairs ? (double)pairs_ok / (double)pairs : 1.0;
+                double v = 0.0;
+                switch (lane) {
+                    case 0: v = head_len / 16.0; break;
+                    case 1: v = k / 32.0; break;
+                    case 2: v = n_rest / 64.0; break;
+                    case 3: v = (double)supc / (double)lmax(1, p.n_bits); break;
+                    case 4: v = log2(1.0 + supc) / 24.0; break;
+                    case 5: v = mn; break;
+                    case 6: v = mean; break;
+                    case 7: v = mx; break;
+                    case 8: v = fmin(mn * supc / minc_d, 8.0) / 8.0; break;
+                    case 9: v = exp(logprod); break;
+                    case 10: v = fmax(-8.0, fmin(8.0, logprod + log(supc / minc_d))) / 8.0; break;
+                    case 11: v = pf; break;
+                    case 12: v = (n_rest - k) / 64.0; break;
+                    case 13: v = minc_d / (double)lmax(1, p.n_bits); break;
+                    case 14: v = fmin(supc / minc_d, 64.0) / 64.0; break;
+                    case 15: v = sqrt(var); break;
+                    case 16: v = k > 1 ? mn2 : mn; break;
+                    case 17: v = (double)gt90 / k; break;
+                    case 18: v = (double)gt99 / k; break;
+                    case 19: v = log2(1.0 + k) / 6.0; break;
+                    case 20: v = n_eq / 8.0; break;
+                    case 21: v = nT / 64.0; break;
+                    case 22: v = (double)i / (double)max(1, nT); break;
+                    case 23: v = top_child ? 1.0 : 0.0; break;
+                    default: v = 0.0;
+                }
+                feat = (float)v;
+                if (p.la_mode == 2 && p.mlp_w) {
+                    const float prob = warp_mlp(p, feat, lane);
+                    if (prob < p.proposal_threshold) {
+                        issue = false;
+                        if (lane == 0) atomicAdd(&st->skipped, 1ull);
+                    }
+                }
+            }
+        }
+    }
+    if (issue && p.log_on) {
+        if (lane == 0) log_idx = atomicAdd(&st->log_n, 1);
+        log_idx = __shfl_sync(0xffffffffu, log_idx, 0);
+        p.log_feat[(int64_t)log_idx * 32 + lane] = feat;
+        if (lane == 0) p.log_label[log_idx] = 0.f;
+    }
+    // the child record
+    if (lane == 0) {
+        DFam ch;
+        ch.slot = cslot; ch.item = citem; ch.head_off = hoff; ch.head_len = head_len;
+        ch.F_off = foff; ch.nF = n_rest; ch.nT = n_tail; ch.sup = supc;
+        ch.next_row = 0; ch.rows_done = 0; ch.state = issue ? 1 : 0; ch.top = 0;
+        p.fams[fid] = ch;
+    }
+    if (issue) {
+        int32_t ls = 0;
+        if (lane == 0) ls = pop_slot(p);
+        ls = __shfl_sync(0xffffffffu, ls, 0);
+        // mask of head + tail: child base & the tail rows
+        if (cslot >= 0) warp_build_mask(p, ls, cslot, -1, -1, Fc, n_tail, lane);
+        else warp_build_mask(p, ls, -1, citem, -1, Fc, n_tail, lane);
+        if (lane == 0) {
+            const int32_t q = atomicAdd(&st->look_n, 1);
+            p.looks[q] = DLook{fid, ls, log_idx, 0};
+            atomicAdd(&st->lookaheads, 1ull);
+        }
+    } else if (lane == 0) {
+        const int32_t k = atomicAdd(&st->stack_n, 1);
+        p.stack[k] = fid;
+    }
+    __syncwarp();
+    finish_row(p, fp, lane);
+}
+
+// ---------------------------------------------------------------------------------- host
+struct Pool {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+int grow(Pool& b, size_t need, cudaStream_t s) {
+    if (need <= b.bytes && b.p) return TFIM_OK;
+    size_t cap = std::max<size_t>(need + need / 2, 1 << 16);
+    void* np = nullptr;
+    TFIM_TRY(dev_alloc(&np, cap, s));
+    if (b.p && b.bytes) TFIM_CUDA(cudaMemcpyAsync(np, b.p, b.bytes, cudaMemcpyDeviceToDevice, s));
+    dev_free(b.p, s);
+    b.p = np;
+    b.bytes = cap;
+    return TFIM_OK;
+}
+
+}  // namespace
+
+struct ResidentState {
+    Pool fams, items, heads, stack, looks, free_slots, defer, mfi_off, mfi_len, mfi_sup, mfi_items, log_feat, log_label;
+    Pool djobs, jobs, rows, row_job, row_local, tiles_l3, tiles_b1, counts, status, is_root, dense_freq, top_pos, top_diag;
+    HostBuf h_status;
+    void release(cudaStream_t s) {
+        for (Pool* b : {&fams, &items, &heads, &stack, &looks, &free_slots, &defer, &mfi_off, &mfi_len, &mfi_sup, &mfi_items,
+                        &log_feat, &log_label, &djobs, &jobs, &rows, &row_job, &row_local, &tiles_l3, &tiles_b1, &counts,
+                        &status, &is_root, &dense_freq, &top_pos, &top_diag}) {
+            dev_free(b->p, s);
+            b->p = nullptr;
+            b->bytes = 0;
+        }
+        h_status.release();
+    }
+};
+
+void free_resident(ResidentState* r, cudaStream_t s) {
+    if (!r) return;
+    r->release(s);
+    delete r;
+}
+
+int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
+    cudaStream_t s = c->stream;
+    const int32_t d = c->n_counted;
+    const int32_t minc = c->info.min_count;
+    const int64_t W = c->W;
+    const int32_t la_mode = o->lookahead;
+    TFIM_CHECK(la_mode != 2 || c->proposal, TFIM_E_STATE, "lookahead mode 2 needs a proposal network (tfim_set_proposal)");
+    if (!c->resident) c->resident = new ResidentState();
+    ResidentState& R = *c->resident;
+    c->la_feats.clear();
+    c->la_labels.clear();
+
+    // the parked id 0 used as a root: the reference's search for that root (host driver)
+    std::vector<char> is_root((size_t)c->info.n_dense + 1, 0);
+    for (int32_t r : c->roots) is_root[r] = 1;
+    if (c->info.n_dense > d && is_root[d]) TFIM_TRY(mine_plain_roots(c, {d}, stt));
+
+    // top family: the counted items frequent by bitmap support, increasing support
+    std::vector<int32_t> F0;
+    for (int32_t e = 0; e < d; e++)
+        if (c->bit_support[e] >= minc) F0.push_back(e);
+    std::stable_sort(F0.begin(), F0.end(), [&](int32_t a, int32_t b) { return c->bit_support[a] < c->bit_support[b]; });
+    const int32_t n0 = (int32_t)F0.size();
+    if (n0 == 0) return TFIM_OK;
+
+    int sm_count = 148;
+    {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, dev);
+    }
+    const int32_t wave_rows = o->wave_cap > 0 ? o->wave_cap : 4096;
+    const int64_t top_out = (int64_t)n0 * n0;
+    int64_t cap_out = std::max<int64_t>(top_out, 64LL << 20);
+    int64_t cap_tiles = 1LL << 21;
+    int64_t cap_rows = std::max<int64_t>(wave_rows, n0) + 64;
+
+    // initial capacities
+    int64_t cap_fam = std::max<int64_t>(4 * n0, 1 << 16);
+    int64_t cap_item = std::max<int64_t>(4 * top_out + 2 * n0, 1 << 20);
+    int64_t cap_head = 1 << 20, cap_mfi = 1 << 16, cap_mfi_items = 1 << 20, cap_slots = 1 << 12, cap_log = 1 << 16;
+    TFIM_TRY(grow(R.status, sizeof(ResStatus), s));
+    TFIM_TRY(grow(R.fams, cap_fam * sizeof(DFam), s));
+    TFIM_TRY(grow(R.items, cap_item * 4, s));
+    TFIM_TRY(grow(R.heads, cap_head * 4, s));
+    TFIM_TRY(grow(R.stack, cap_fam * 4, s));
+    TFIM_TRY(grow(R.looks, cap_rows * sizeof(DLook), s));
+    TFIM_TRY(grow(R.free_slots, cap_slots * 4, s));
+    TFIM_TRY(grow(R.defer, cap_slots * 4, s));
+    TFIM_TRY(grow(R.mfi_off, cap_mfi * 4, s));
+    TFIM_TRY(grow(R.mfi_len, cap_mfi * 4, s));
+    TFIM_TRY(grow(R.mfi_sup, cap_mfi * 4, s));
+    TFIM_TRY(grow(R.mfi_items, cap_mfi_items * 4, s));
+    if (o->log_lookahead) {
+        TFIM_TRY(grow(R.log_feat, cap_log * 32 * 4, s));
+        TFIM_TRY(grow(R.log_label, cap_log * 4, s));
+    }
+    TFIM_TRY(grow(R.djobs, cap_rows * sizeof(DJob), s));
+    TFIM_TRY(grow(R.jobs, cap_rows * sizeof(JobDesc), s));
+    TFIM_TRY(grow(R.rows, cap_rows * sizeof(RowDesc), s));
+    TFIM_TRY(grow(R.row_job, cap_rows * 4, s));
+    TFIM_TRY(grow(R.row_local, cap_rows * 4, s));
+    TFIM_TRY(grow(R.tiles_l3, cap_tiles * sizeof(TileDesc), s));
+    TFIM_TRY(grow(R.tiles_b1, cap_tiles * sizeof(TileDesc), s));
+    TFIM_TRY(grow(R.counts, cap_out * 4, s));
+    TFIM_TRY(grow(R.is_root, is_root.size(), s));
+    TFIM_TRY(grow(R.dense_freq, (size_t)std::max<int32_t>(c->info.n_dense, 1) * 4, s));
+    TFIM_TRY(grow(R.top_pos, (size_t)std::max<int32_t>(c->info.n_dense, 1) * 4, s));
+    TFIM_TRY(grow(R.top_diag, (size_t)n0 * 4, s));
+    TFIM_CUDA(cudaMemcpyAsync(R.is_root.p, is_root.data(), is_root.size(), cudaMemcpyHostToDevice, s));
+    TFIM_CUDA(cudaMemcpyAsync(R.dense_freq.p, c->dense_freq.data(), c->dense_freq.size() * 4, cudaMemcpyHostToDevice, s));
+    // mask slots (grown on demand)
+    int64_t slot_cap = c->d_masks.bytes / ((size_t)W * 4);
+
+    // the top family record and its single job
+    DFam top;
+    top.slot = -1; top.item = -1; top.head_off = 0; top.head_len = 0; top.F_off = 0; top.nF = n0; top.nT = n0;
+    top.sup = 0; top.next_row = n0; top.rows_done = 0; top.state = 0; top.top = 1;
+    TFIM_CUDA(cudaMemcpyAsync(R.fams.p, &top, sizeof top, cudaMemcpyHostToDevice, s));
+    TFIM_CUDA(cudaMemcpyAsync(R.items.p, F0.data(), (size_t)n0 * 4, cudaMemcpyHostToDevice, s));
+    ResStatus hs;
+    memset(&hs, 0, sizeof hs);
+    hs.fam_n = 1;
+    hs.item_n = n0;
+    hs.jobs = 1;
+    hs.rows = n0;
+    hs.out_total = top_out;
+    hs.max_cols = n0;
+    hs.nodes = n0;
+    hs.supports = (unsigned long long)top_out;
+    {
+        std::vector<DJob> dj(1);
+        dj[0] = DJob{0, kJobFam, 0, n0, -1, -1, 0, 0};
+        std::vector<JobDesc> jd(1);
+        jd[0] = JobDesc{-1, -1, n0, n0, 0, 0, 0, -1, 0};
+        std::vector<RowDesc> rows(n0);
+        std::vector<int32_t> rj(n0, 0), rl(n0);
+        for (int32_t k = 0; k < n0; k++) { rows[k] = RowDesc{-1, F0[k]}; rl[k] = k; }
+        TFIM_CUDA(cudaMemcpyAsync(R.djobs.p, dj.data(), sizeof(DJob), cudaMemcpyHostToDevice, s));
+        TFIM_CUDA(cudaMemcpyAsync(R.jobs.p, jd.data(), sizeof(JobDesc), cudaMemcpyHostToDevice, s));
+        TFIM_CUDA(cudaMemcpyAsync(R.rows.p, rows.data(), (size_t)n0 * sizeof(RowDesc), cudaMemcpyHostToDevice, s));
+        TFIM_CUDA(cudaMemcpyAsync(R.row_job.p, rj.data(), (size_t)n0 * 4, cudaMemcpyHostToDevice, s));
+        TFIM_CUDA(cudaMemcpyAsync(R.row_local.p, rl.data(), (size_t)n0 * 4, cudaMemcpyHostToDevice, s));
+        std::vector<int32_t> pos((size_t)std::max<int32_t>(c->info.n_dense, 1), -1), diag(n0);
+        for (int32_t k = 0; k < n0; k++) { pos[F0[k]] = k; diag[k] = c->bit_support[F0[k]]; }
+        TFIM_CUDA(cudaMemcpyAsync(R.top_pos.p, pos.data(), pos.size() * 4, cudaMemcpyHostToDevice, s));
+        TFIM_CUDA(cudaMemcpyAsync(R.top_diag.p, diag.data(), (size_t)n0 * 4, cudaMemcpyHostToDevice, s));
+    }
+    TFIM_CUDA(cudaMemcpyAsync(R.status.p, &hs, sizeof hs, cudaMemcpyHostToDevice, s));
+    TFIM_TRY(R.h_status.reserve(sizeof(ResStatus)));
+    ResStatus* hst = R.h_status.as<ResStatus>();
+
+    // top family counting: pair co-occurrence or the symmetric bitmap Gram (cost model)
+    int top_mode;
+    {
+        const double nF = n0;
+        const bool b1 = o->counter != TFIM_COUNTER_LOP3 && (o->counter == TFIM_COUNTER_TENSOR || nF >= 16);
+        const double bitmap_s = nF * nF * (double)c->n_bits / 2.0 / (b1 ? kTuneB1BitOps : kTuneLop3BitOps);
+        const double pairs_s = c->red_pair_work / 2.0 / kTunePairIncrements + nF * nF * 4.0 / kTuneHbmBytes;
+        if (o->top_counter == 1) top_mode = 1;
+        else if (o->top_counter == 2) top_mode = c->d_red_off ? 2 : 1;
+        else top_mode = (c->d_red_off && pairs_s < bitmap_s) ? 2 : 1;
+    }
+    const bool top_b1 = o->counter == TFIM_COUNTER_TENSOR || (o->counter != TFIM_COUNTER_LOP3 && n0 >= 16);
+
+    const double t_host0 = std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+    double sync_ms = 0, kernel_ms = 0;
+    int64_t launches = 0, count_launches = 0, bytes_alg = 0, waves = 0;
+    const int64_t row_bytes = (c->n_bits + 7) / 8;
+
+    ResPtrs P;
+    auto refresh_ptrs = [&]() {
+        P.fams = (DFam*)R.fams.p; P.items = (int32_t*)R.items.p; P.heads = (int32_t*)R.heads.p;
+        P.stack = (int32_t*)R.stack.p; P.looks = (DLook*)R.looks.p; P.free_slots = (int32_t*)R.free_slots.p;
+        P.defer = (int32_t*)R.defer.p; P.mfi_off = (int32_t*)R.mfi_off.p; P.mfi_len = (int32_t*)R.mfi_len.p;
+        P.mfi_sup = (int32_t*)R.mfi_sup.p; P.mfi_items = (int32_t*)R.mfi_items.p;
+        P.log_feat = (float*)R.log_feat.p; P.log_label = (float*)R.log_label.p;
+        P.djobs = (DJob*)R.djobs.p; P.jobs = (JobDesc*)R.jobs.p; P.rows = (RowDesc*)R.rows.p;
+        P.row_job = (int32_t*)R.row_job.p; P.row_local = (int32_t*)R.row_local.p;
+        P.tiles_l3 = (TileDesc*)R.tiles_l3.p; P.tiles_b1 = (TileDesc*)R.tiles_b1.p; P.counts = (int32_t*)R.counts.p;
+        P.bitmap = c->d_bitmap; P.masks = c->d_masks.as<uint32_t>(); P.dense_freq = (const int32_t*)R.dense_freq.p;
+        P.is_root = (const uint8_t*)R.is_root.p; P.st = (ResStatus*)R.status.p;
+        P.W = W; P.n_bits = c->n_bits; P.min_count = minc; P.wave_rows = wave_rows;
+        P.cap_out = cap_out; P.cap_tiles = cap_tiles; P.counter = o->counter; P.la_mode = la_mode;
+        P.log_on = o->log_lookahead; P.proposal_threshold = c->proposal_threshold; P.kslice_min = 64; P.sm_count = sm_count;
+        P.mlp_w = nullptr; P.mlp_p = nullptr;
+        if (la_mode == 2 && c->proposal) {
+            const void* wb = nullptr;
+            const float* pp = nullptr;
+            mlp_device_params(c->proposal, &wb, &pp);
+            P.mlp_w = (const __nv_bfloat16*)wb;
+            P.mlp_p = pp;
+        }
+    };
+    // capacity for the worst case of one expand over `rows` rows of at most `max_cols`
+    // columns each and `out_total` counts
+    auto ensure = [&](const ResStatus& h) -> int {
+        const int64_t rows = h.rows;
+        const int64_t need_fam = h.fam_n + rows + 1;
+        const int64_t need_item = h.item_n + 2 * h.out_total + rows + 1;
+        const int64_t need_head = h.head_n + rows * (int64_t)(h.max_head + 2 + h.max_cols) + 1;
+        const int64_t need_mfi = h.mfi_n + rows + h.jobs + 1;
+        const int64_t need_mfi_items = h.mfi_item_n + (rows + h.jobs) * (int64_t)(h.max_head + 2 + h.max_cols) + 1;
+        const int64_t need_slots = h.slot_n + 2 * rows + 2;
+        const int64_t need_log = h.log_n + rows + 1;
+        TFIM_TRY(grow(R.fams, need_fam * sizeof(DFam), s));
+        TFIM_TRY(grow(R.stack, need_fam * 4, s));
+        TFIM_TRY(grow(R.items, need_item * 4, s));
+        TFIM_TRY(grow(R.heads, need_head * 4, s));
+        TFIM_TRY(grow(R.mfi_off, need_mfi * 4, s));
+        TFIM_TRY(grow(R.mfi_len, need_mfi * 4, s));
+        TFIM_TRY(grow(R.mfi_sup, need_mfi * 4, s));
+        TFIM_TRY(grow(R.mfi_items, need_mfi_items * 4, s));
+        TFIM_TRY(grow(R.looks, (rows + 1) * sizeof(DLook), s));
+        TFIM_TRY(grow(R.free_slots, need_slots * 4, s));
+        TFIM_TRY(grow(R.defer, need_slots * 4, s));
+        if (o->log_lookahead) {
+            TFIM_TRY(grow(R.log_feat, need_log * 32 * 4, s));
+            TFIM_TRY(grow(R.log_label, need_log * 4, s));
+        }
+        if (need_slots > slot_cap) {
+            DevBuf nb;
+            nb.stream = s;
+            const int64_t ncap = std::max<int64_t>(need_slots + need_slots / 2, 64);
+            TFIM_TRY(nb.reserve((size_t)ncap * (size_t)W * 4));
+            if (c->d_masks.p && slot_cap > 0)
+                TFIM_CUDA(cudaMemcpyAsync(nb.p, c->d_masks.p, (size_t)slot_cap * (size_t)W * 4, cudaMemcpyDeviceToDevice, s));
+            c->d_masks.release();
+            c->d_masks = nb;
+            slot_cap = ncap;
+        }
+        refresh_ptrs();
+        return TFIM_OK;
+    };
+
+    // wave 1: the top family, counted whole
+    *hst = hs;
+    TFIM_TRY(ensure(hs));
+    {
+        std::vector<TileDesc> tl;
+        if (top_mode == 1) {
+            if (top_b1) {
+                const int64_t base = (int64_t)((n0 + kB1Rows - 1) / kB1Rows) * ((n0 + kB1Cols - 1) / kB1Cols);
+                int64_t ks = std::min<int64_t>(std::max<int64_t>(1, (4LL * sm_count + base - 1) / base), W / 64);
+                const int64_t kslice = ((W / 64 + ks - 1) / ks) * 64;
+                tiles_b1(0, n0, n0, W, kslice, tl, true);
+            } else {
+                const int64_t base = (int64_t)((n0 + kLop3Rows - 1) / kLop3Rows) * ((n0 + 63) / 64);
+                int64_t ws = std::min<int64_t>(std::max<int64_t>(1, (8LL * sm_count + base - 1) / base), std::max<int64_t>(1, W / 256));
+                const int64_t wslice = ((W / 64 + ws - 1) / ws) * 64;
+                tiles_lop3(0, n0, n0, W, wslice, tl, true);
+            }
+        }
+        if ((int64_t)tl.size() > cap_tiles) {
+            cap_tiles = (int64_t)tl.size();
+            TFIM_TRY(grow(R.tiles_l3, cap_tiles * sizeof(TileDesc), s));
+            TFIM_TRY(grow(R.tiles_b1, cap_tiles * sizeof(TileDesc), s));
+            refresh_ptrs();
+        }
+        if (!tl.empty())
+            TFIM_CUDA(cudaMemcpyAsync(top_b1 ? R.tiles_b1.p : R.tiles_l3.p, tl.data(), tl.size() * sizeof(TileDesc),
+                                      cudaMemcpyHostToDevice, s));
+        TFIM_CUDA(cudaMemsetAsync(R.counts.p, 0, (size_t)top_out * 4, s));
+        CountArgs a;
+        a.bitmap = c->d_bitmap; a.W = W; a.masks = c->d_masks.as<uint32_t>(); a.jobs = P.jobs; a.rows = P.rows;
+        a.cols = P.items; a.out = P.counts;
+        TFIM_CUDA(cudaEventRecord(c->ev0, s));
+        if (top_mode == 2) {
+            TFIM_TRY(launch_pair_count(c->d_red_off, c->d_red_items, c->n_bits, (const int32_t*)R.top_pos.p, n0, P.counts, s));
+            bytes_alg += (c->n_bits + 1) * 8 + c->n_red_items * 4 + 4 * top_out;
+        } else {
+            a.tiles = top_b1 ? P.tiles_b1 : P.tiles_l3;
+            a.n_tiles = (int32_t)tl.size();
+            TFIM_TRY(top_b1 ? launch_count_b1(a, s) : launch_count_lop3(a, s));
+            bytes_alg += row_bytes * 2 * n0 + 4 * top_out;
+        }
+        TFIM_CUDA(cudaEventRecord(c->ev1, s));
+        TFIM_TRY(launch_mirror(P.counts, n0, top_mode == 2 ? (const int32_t*)R.top_diag.p : nullptr, s));
+        launches += 2;
+        count_launches++;
+        const int64_t threads = (int64_t)n0 * 32;
+        k_res_expand<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(P);
+        TFIM_CUDA(cudaGetLastError());
+        launches++;
+        waves++;
+        float ms = 0;
+        TFIM_CUDA(cudaEventSynchronize(c->ev1));
+        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+        kernel_ms += ms;
+    }
+    // following waves
+    while (true) {
+        k_res_pack<<<1, kPackThreads, 0, s>>>(P);
+        TFIM_CUDA(cudaGetLastError());
+        launches++;
+        TFIM_CUDA(cudaMemcpyAsync(hst, R.status.p, sizeof(ResStatus), cudaMemcpyDeviceToHost, s));
+        const double ts = std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+        TFIM_CUDA(cudaStreamSynchronize(s));
+        sync_ms += (std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count() - ts) * 1e3;
+        TFIM_CHECK(hst->error == 0, TFIM_E_STATE, "resident search invariant failed (code %d)", hst->error);
+        if (hst->starved) {
+            // a single row does not fit the count buffer: enlarge it and retry the pack
+            cap_out *= 4;
+            TFIM_TRY(grow(R.counts, cap_out * 4, s));
+            hst->starved = 0;
+            TFIM_CUDA(cudaMemcpyAsync(R.status.p, hst, sizeof(ResStatus), cudaMemcpyHostToDevice, s));
+            refresh_ptrs();
+            continue;
+        }
+        if (hst->jobs == 0) break;
+        TFIM_TRY(ensure(*hst));
+        TFIM_CUDA(cudaMemsetAsync(R.counts.p, 0, (size_t)hst->out_total * 4, s));
+        CountArgs a;
+        a.bitmap = c->d_bitmap; a.W = W; a.masks = c->d_masks.as<uint32_t>(); a.jobs = P.jobs; a.rows = P.rows;
+        a.cols = P.items; a.out = P.counts;
+        TFIM_CUDA(cudaEventRecord(c->ev0, s));
+        if (hst->tiles_l3) {
+            a.tiles = P.tiles_l3;
+            a.n_tiles = hst->tiles_l3;
+            TFIM_TRY(launch_count_lop3(a, s));
+            launches++;
+            count_launches++;
+        }
+        if (hst->tiles_b1) {
+            a.tiles = P.tiles_b1;
+            a.n_tiles = hst->tiles_b1;
+            TFIM_TRY(launch_count_b1(a, s));
+            launches++;
+            count_launches++;
+        }
+        TFIM_CUDA(cudaEventRecord(c->ev1, s));
+        bytes_alg += row_bytes * (2LL * hst->rows + hst->jobs) + 4 * hst->out_total;   // rows, columns ~ rows, bases
+        const int64_t threads = (int64_t)hst->rows * 32;
+        k_res_expand<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(P);
+        TFIM_CUDA(cudaGetLastError());
+        launches++;
+        waves++;
+        float ms = 0;
+        TFIM_CUDA(cudaEventSynchronize(c->ev1));
+        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+        kernel_ms += ms;
+    }
+    // results
+    const ResStatus fin = *hst;
+    std::vector<int32_t> moff(fin.mfi_n), mlen(fin.mfi_n), msup(fin.mfi_n), mitems(fin.mfi_item_n);
+    if (fin.mfi_n) {
+        TFIM_CUDA(cudaMemcpyAsync(moff.data(), R.mfi_off.p, (size_t)fin.mfi_n * 4, cudaMemcpyDeviceToHost, s));
+        TFIM_CUDA(cudaMemcpyAsync(mlen.data(), R.mfi_len.p, (size_t)fin.mfi_n * 4, cudaMemcpyDeviceToHost, s));
+        TFIM_CUDA(cudaMemcpyAsync(msup.data(), R.mfi_sup.p, (size_t)fin.mfi_n * 4, cudaMemcpyDeviceToHost, s));
+        TFIM_CUDA(cudaMemcpyAsync(mitems.data(), R.mfi_items.p, (size_t)fin.mfi_item_n * 4, cudaMemcpyDeviceToHost, s));
+    }
+    if (o->log_lookahead && fin.log_n) {
+        c->la_feats.resize((size_t)fin.log_n * 32);
+        c->la_labels.resize(fin.log_n);
+        TFIM_CUDA(cudaMemcpyAsync(c->la_feats.data(), R.log_feat.p, (size_t)fin.log_n * 32 * 4, cudaMemcpyDeviceToHost, s));
+        TFIM_CUDA(cudaMemcpyAsync(c->la_labels.data(), R.log_label.p, (size_t)fin.log_n * 4, cudaMemcpyDeviceToHost, s));
+    }
+    TFIM_CUDA(cudaStreamSynchronize(s));
+    for (int32_t k = 0; k < fin.mfi_n; k++) {
+        std::vector<int32_t> it(mitems.begin() + moff[k], mitems.begin() + moff[k] + mlen[k]);
+        std::sort(it.begin(), it.end(), std::greater<int32_t>());
+        c->mfi_items.push_back(std::move(it));
+        c->mfi_support.push_back(msup[k]);
+    }
+    stt->nodes += (int64_t)fin.nodes;
+    stt->supports += (int64_t)fin.supports;
+    stt->lookaheads += (int64_t)fin.lookaheads;
+    stt->lookahead_hits += (int64_t)fin.hits;
+    stt->lookaheads_skipped += (int64_t)fin.skipped;
+    stt->pruned_pep += (int64_t)fin.pep;
+    stt->waves += waves;
+    stt->launches += launches;
+    stt->count_launches += count_launches;
+    stt->kernel_ms += kernel_ms;
+    stt->sync_ms += sync_ms;
+    stt->bytes_alg += bytes_alg;
+    stt->bit_ops = stt->supports * c->n_bits;
+    (void)t_host0;
+    return TFIM_OK;
+}
+
+}  // namespace tfim

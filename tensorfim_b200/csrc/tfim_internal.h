@@ -89,6 +89,8 @@ struct JobDesc {
     int32_t row_off;      // into the RowDesc table
     int32_t col_off;      // into the column table
     int64_t out_off;      // into the counts buffer
+    int32_t self_col;     // column index that stands for all ones (not read from the table), or -1
+    int32_t pad;
 };
 struct RowDesc {
     int32_t slot;
@@ -154,7 +156,7 @@ int launch_compact(const int32_t* counts, const JobDesc* jobs, const int32_t* ro
 
 }  // namespace tfim
 
-namespace tfim { struct EngineState; }
+namespace tfim { struct EngineState; struct ResidentState; }
 
 // ------------------------------------------------------------------ context
 struct tfim_ctx {
@@ -191,6 +193,7 @@ struct tfim_ctx {
     tfim_mine_stats last_stats{};
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     tfim::EngineState* engine = nullptr;
+    tfim::ResidentState* resident = nullptr;
     // learned lookahead proposal (not owned) and the outcome log of the last mine
     tfim_mlp* proposal = nullptr;
     float proposal_threshold = 0.5f;
@@ -199,9 +202,19 @@ struct tfim_ctx {
 };
 
 namespace tfim {
+// Tile lists of one count job (mine.cu).  `upper`: rows and columns are the same list and
+// only tiles holding some (i, j >= i) are emitted.
+void tiles_lop3(int32_t job, int32_t nr, int32_t nc, int64_t W, int64_t wslice, std::vector<TileDesc>& out,
+                bool upper = false);
+void tiles_b1(int32_t job, int32_t nr, int32_t nc, int64_t W, int64_t kslice, std::vector<TileDesc>& out,
+              bool upper = false);
 struct EngineState;                        // persistent buffers of the search drivers (mine.cu)
 void free_engine(EngineState* e);
 int mine_plain(tfim_ctx* ctx, const tfim_mine_opts* o, tfim_mine_stats* st);
 int mine_batched(tfim_ctx* ctx, const tfim_mine_opts* o, tfim_mine_stats* st);
+int mine_resident(tfim_ctx* ctx, const tfim_mine_opts* o, tfim_mine_stats* st);
+int mine_plain_roots(tfim_ctx* ctx, const std::vector<int32_t>& roots, tfim_mine_stats* st);
+void free_resident(ResidentState* r, cudaStream_t s);
+int mlp_device_params(tfim_mlp* h, const void** wbf, const float** params);
 int compute_bit_supports(tfim_ctx* ctx);
 }  // namespace tfim

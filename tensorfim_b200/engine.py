@@ -18,7 +18,7 @@ import numpy as np
 from . import _lib
 from ._lib import TfimError, check, lib
 
-ENGINES = {"plain": _lib.ENGINE_PLAIN, "batched": _lib.ENGINE_BATCHED}
+ENGINES = {"plain": _lib.ENGINE_PLAIN, "batched": _lib.ENGINE_BATCHED, "resident": _lib.ENGINE_RESIDENT}
 COUNTERS = {"auto": _lib.COUNTER_AUTO, "lop3": _lib.COUNTER_LOP3, "tensor": _lib.COUNTER_TENSOR}
 
 

@@ -1,6 +1,7 @@
 """One mine of a seeded benchmark database, for profiler captures.
 
-    python -m tensorfim_b200.profcase --cfg 4 --scale 0.25 --counter tensor [--engine batched] [--top auto]
+    python -m tensorfim_b200.profcase --cfg 4 --scale 0.25 --counter tensor [--engine batched|resident|plain]
+                                      [--top auto|bitmap|pairs] [--lookahead off|filtered|learned|all]
 
 Generates the configuration's database (tensorfim_b200.synth) at the given row scale,
 builds it on cuda:0 and mines it once; prints the MFI count and the engine statistics.
@@ -22,6 +23,7 @@ def main() -> None:
     ap.add_argument("--engine", default="batched")
     ap.add_argument("--counter", default="auto")
     ap.add_argument("--top", default="auto")
+    ap.add_argument("--lookahead", default="learned", choices=["off", "filtered", "learned", "all"])
     ap.add_argument("--repeat", type=int, default=1)
     a = ap.parse_args()
     kw = {"scale": a.scale} if a.cfg != 3 else {"scale": a.scale, "replicas": 1}
@@ -29,7 +31,7 @@ def main() -> None:
     minsup = a.minsup if a.minsup is not None else MINSUP[a.cfg]
     with Database.from_csr(db0.offsets, db0.items, minsup) as db:
         for _ in range(a.repeat):
-            r = db.mine(engine=a.engine, counter=a.counter, top=a.top)
+            r = db.mine(engine=a.engine, counter=a.counter, top=a.top, lookahead=a.lookahead)
         print(json.dumps({"mfis": len(r.mfis), "info": db.info, "stats": r.stats}))
 
 

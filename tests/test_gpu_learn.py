@@ -69,13 +69,15 @@ def test_learned_lookahead_keeps_output_identical(tmp_path, name):
             for thr in (0.0, 0.5, 1.01):
                 db.set_proposal(prop, thr)
                 assert db.mine(lookahead="learned").as_dict() == fx["expected"]
+                assert db.mine(engine="resident", lookahead="learned").as_dict() == fx["expected"]
 
 
-def test_lookahead_log_records_outcomes(tmp_path):
+@pytest.mark.parametrize("engine", ["batched", "resident"])
+def test_lookahead_log_records_outcomes(tmp_path, engine):
     fx = load_golden("cfg1_full")
     path = golden_input(fx, tmp_path)
     with tf.Database.from_file(path, 0.10) as db:
-        r = db.mine(lookahead="filtered", log_lookahead=True)
+        r = db.mine(engine=engine, lookahead="filtered", log_lookahead=True)
         x, y = db.lookahead_log()
         assert x.shape == (r.stats["lookaheads"], 32)
         assert int(y.sum()) == r.stats["lookahead_hits"]

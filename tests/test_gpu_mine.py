@@ -23,6 +23,11 @@ VARIANTS = [
     dict(engine="batched", counter="auto", lookahead=True, top="pairs"),
     dict(engine="batched", counter="lop3", lookahead=False, top="bitmap"),
     dict(engine="batched", counter="tensor", lookahead=True, top="bitmap"),
+    dict(engine="resident", counter="auto", lookahead=True),
+    dict(engine="resident", counter="lop3", lookahead=False, top="bitmap"),
+    dict(engine="resident", counter="tensor", lookahead=True, top="bitmap"),
+    dict(engine="resident", counter="auto", lookahead="all", wave_cap=37),
+    dict(engine="resident", counter="auto", lookahead=True, top="pairs"),
 ]
 PLAIN_OK = {"cfg1_full", "cfg2_full", "cfg3_base", "cfg3_base_t30", "cfg4_s001", "cfg5_s002", "edge_dups",
             "edge_format", "edge_identical", "edge_item0", "edge_none", "edge_single", "edge_ties"}
@@ -106,6 +111,8 @@ def test_cfg4_full_size_certified():
         res = db.mine()
         assert len(res.mfis) > 1000
         _certify(db, res.mfis, db.dense_to_orig())
+        assert db.mine(engine="resident").as_dict() == res.as_dict()
+        assert db.mine(engine="resident", lookahead="learned").as_dict() == res.as_dict()
 
 
 @pytest.mark.slow
