@@ -44,6 +44,8 @@ typedef struct tfim_ctx tfim_ctx;
 #define TFIM_COUNTER_AUTO    0   /* chosen per job from its shape */
 #define TFIM_COUNTER_LOP3    1   /* AND + popc on CUDA cores */
 #define TFIM_COUNTER_TENSOR  2   /* b1 AND+POPC tensor-core MMA */
+#define TFIM_COUNTER_PROJ    3   /* resident engine: projected counting (prefix transactions x
+                                    the reduced transaction list) wherever it applies, else auto */
 
 TFIM_API const char* tfim_version(void);
 TFIM_API const char* tfim_last_error(void);

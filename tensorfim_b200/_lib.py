@@ -27,6 +27,7 @@ ENGINE_RESIDENT = 2
 COUNTER_AUTO = 0
 COUNTER_LOP3 = 1
 COUNTER_TENSOR = 2
+COUNTER_PROJ = 3
 
 # every entry point declared in include/tfim.h
 EXPORTS = [

@@ -192,6 +192,7 @@ int tfim_dense_freq(const tfim_ctx* c, int32_t* out) {
 int tfim_set_counter(tfim_ctx* c, int32_t counter) {
     TFIM_CHECK(c, TFIM_E_INVALID, "null context");
     TFIM_CHECK(counter >= TFIM_COUNTER_AUTO && counter <= TFIM_COUNTER_TENSOR, TFIM_E_INVALID, "unknown counter %d", counter);
+    // (TFIM_COUNTER_PROJ applies to the search's family counts only)
     c->counter_pref = counter;
     return TFIM_OK;
 }

@@ -197,14 +197,21 @@ int grid_for(int64_t n, int per = 256) {
 }  // namespace
 
 int compute_bit_supports(tfim_ctx* c) {
-    c->bit_support.assign(c->n_counted, 0);
-    if (c->n_counted == 0) return TFIM_OK;
-    TFIM_TRY(c->d_scratch[7].reserve((size_t)c->n_counted * 4));
-    k_row_popc<<<c->n_counted, 256, 0, c->stream>>>(c->d_bitmap, c->W, c->n_counted, c->d_scratch[7].as<int32_t>());
-    TFIM_CUDA(cudaGetLastError());
-    TFIM_CUDA(cudaMemcpyAsync(c->bit_support.data(), c->d_scratch[7].p, (size_t)c->n_counted * 4,
-                              cudaMemcpyDeviceToHost, c->stream));
-    TFIM_CUDA(cudaStreamSynchronize(c->stream));
+    // popcount of every bitmap row (the counted ones are the bitmap supports); their sum
+    // equals the reduced transaction list's length exactly when no row repeats an id
+    const int32_t rows = c->from_db ? c->info.n_dense : c->n_counted;
+    std::vector<int32_t> all(std::max<int32_t>(rows, 0), 0);
+    if (rows > 0) {
+        TFIM_TRY(c->d_scratch[7].reserve((size_t)rows * 4));
+        k_row_popc<<<rows, 256, 0, c->stream>>>(c->d_bitmap, c->W, rows, c->d_scratch[7].as<int32_t>());
+        TFIM_CUDA(cudaGetLastError());
+        TFIM_CUDA(cudaMemcpyAsync(all.data(), c->d_scratch[7].p, (size_t)rows * 4, cudaMemcpyDeviceToHost, c->stream));
+        TFIM_CUDA(cudaStreamSynchronize(c->stream));
+    }
+    c->bit_support.assign(all.begin(), all.begin() + std::min<int32_t>(rows, c->n_counted));
+    int64_t total = 0;
+    for (int32_t v : all) total += v;
+    c->csr_exact = c->from_db && c->d_red_off && total == c->n_red_items;
     return TFIM_OK;
 }
 

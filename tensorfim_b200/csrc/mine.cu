@@ -596,8 +596,8 @@ int mine_batched(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* st) {
         const double pairs_s = c->red_pair_work / 2.0 / kTunePairIncrements + nF * nF * 4.0 / kTuneHbmBytes;
         if (fits) {
             if (o->top_counter == 1) top_mode = 1;
-            else if (o->top_counter == 2) top_mode = c->d_red_off ? 2 : 1;
-            else top_mode = (c->d_red_off && pairs_s < bitmap_s) ? 2 : 1;
+            else if (o->top_counter == 2) top_mode = c->csr_exact ? 2 : 1;
+            else top_mode = (c->csr_exact && pairs_s < bitmap_s) ? 2 : 1;
         }
     }
     auto use_b1_for = [&](int32_t nr, int32_t nc) {

@@ -51,7 +51,7 @@ struct DJob {
 
 struct ResStatus {
     int32_t stack_n, look_n, fam_n, item_n, head_n, mfi_n, mfi_item_n, slot_n, free_n, free_taken, defer_n, log_n;
-    int32_t jobs, rows, tiles_l3, tiles_b1;
+    int32_t jobs, rows, tiles_l3, tiles_b1, n_proj, pad0;
     int64_t out_total;
     int32_t max_cols, max_head, starved, error;
     unsigned long long supports, nodes, lookaheads, hits, skipped, pep;
@@ -99,7 +99,23 @@ struct ResPtrs {
     float proposal_threshold;
     int64_t kslice_min;           // b1 word slice when tiles are few (multiple of 64)
     int32_t sm_count;
+    int32_t* proj_list;           // family jobs counted by the projected counter
+    float avg_len;                // mean reduced transaction length
+    int32_t csr_ok;               // the reduced transaction list repeats no id within a row
 };
+
+// Projected counting pays when the prefix holds few transactions: it walks the base's set
+// bits (W words) and looks up about 6 entries per item of each of its sup transactions,
+// against the bitmap counters' (rows + columns + 1) x W words.
+__device__ __forceinline__ bool use_proj(const ResPtrs& p, const JobDesc& jd, int32_t sup) {
+    if (!p.csr_ok || jd.n_cols > kProjMaxCols || (jd.base_slot >= 0 && jd.base_item >= 0)) return false;
+    if (jd.base_slot < 0 && jd.base_item < 0) return false;
+    if (p.counter == TFIM_COUNTER_PROJ) return true;
+    if (p.counter != TFIM_COUNTER_AUTO) return false;
+    const double proj = (double)p.W + (double)sup * 6.0 * (double)p.avg_len;
+    const double bitmap = (double)(jd.n_rows + jd.n_cols + 1) * (double)p.W;
+    return proj < bitmap;
+}
 
 __host__ __device__ __forceinline__ int64_t lmin(int64_t a, int64_t b) { return a < b ? a : b; }
 __host__ __device__ __forceinline__ int64_t lmax(int64_t a, int64_t b) { return a > b ? a : b; }
@@ -160,6 +176,7 @@ __global__ void __launch_bounds__(kPackThreads) k_res_pack(ResPtrs p) {
     if (tid == 0) {
         s_n_jobs = 0; s_rows_total = 0; s_out_total = 0; s_max_cols = 0; s_max_head = 0; s_done = 0;
         s_stack_after = st->stack_n;
+        st->n_proj = 0;
     }
     __syncthreads();
     if (tid == 0) {
@@ -345,9 +362,16 @@ __global__ void __launch_bounds__(kPackThreads) k_res_pack(ResPtrs p) {
             a3[q] = a1[q] = 0;
             if (j < nj) {
                 const JobDesc jd = p.jobs[j];
-                const bool b1 = use_b1_shape(p, jd.n_rows, jd.n_cols) && p.djobs[j].kind == kJobFam;
-                if (b1) a1[q] = b1_tiles(jd.n_rows, jd.n_cols);
-                else a3[q] = l3_tiles(jd.n_rows, jd.n_cols);
+                const DJob djq = p.djobs[j];
+                const bool fam = djq.kind == kJobFam;
+                if (fam && use_proj(p, jd, p.fams[djq.fam].sup)) {
+                    const int32_t k = atomicAdd(&p.st->n_proj, 1);
+                    p.proj_list[k] = j;
+                } else if (use_b1_shape(p, jd.n_rows, jd.n_cols) && fam) {
+                    a1[q] = b1_tiles(jd.n_rows, jd.n_cols);
+                } else {
+                    a3[q] = l3_tiles(jd.n_rows, jd.n_cols);
+                }
             }
         }
         Scan(tmp.scan).ExclusiveSum(a3, x3, s_agg);
@@ -856,12 +880,13 @@ int grow(Pool& b, size_t need, cudaStream_t s) {
 
 struct ResidentState {
     Pool fams, items, heads, stack, looks, free_slots, defer, mfi_off, mfi_len, mfi_sup, mfi_items, log_feat, log_label;
-    Pool djobs, jobs, rows, row_job, row_local, tiles_l3, tiles_b1, counts, status, is_root, dense_freq, top_pos, top_diag;
+    Pool djobs, jobs, rows, row_job, row_local, tiles_l3, tiles_b1, counts, status, is_root, dense_freq, top_pos, top_diag,
+        proj_list;
     HostBuf h_status;
     void release(cudaStream_t s) {
         for (Pool* b : {&fams, &items, &heads, &stack, &looks, &free_slots, &defer, &mfi_off, &mfi_len, &mfi_sup, &mfi_items,
                         &log_feat, &log_label, &djobs, &jobs, &rows, &row_job, &row_local, &tiles_l3, &tiles_b1, &counts,
-                        &status, &is_root, &dense_freq, &top_pos, &top_diag}) {
+                        &status, &is_root, &dense_freq, &top_pos, &top_diag, &proj_list}) {
             dev_free(b->p, s);
             b->p = nullptr;
             b->bytes = 0;
@@ -938,6 +963,7 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
     TFIM_TRY(grow(R.rows, cap_rows * sizeof(RowDesc), s));
     TFIM_TRY(grow(R.row_job, cap_rows * 4, s));
     TFIM_TRY(grow(R.row_local, cap_rows * 4, s));
+    TFIM_TRY(grow(R.proj_list, cap_rows * 4, s));
     TFIM_TRY(grow(R.tiles_l3, cap_tiles * sizeof(TileDesc), s));
     TFIM_TRY(grow(R.tiles_b1, cap_tiles * sizeof(TileDesc), s));
     TFIM_TRY(grow(R.counts, cap_out * 4, s));
@@ -996,8 +1022,8 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
         const double bitmap_s = nF * nF * (double)c->n_bits / 2.0 / (b1 ? kTuneB1BitOps : kTuneLop3BitOps);
         const double pairs_s = c->red_pair_work / 2.0 / kTunePairIncrements + nF * nF * 4.0 / kTuneHbmBytes;
         if (o->top_counter == 1) top_mode = 1;
-        else if (o->top_counter == 2) top_mode = c->d_red_off ? 2 : 1;
-        else top_mode = (c->d_red_off && pairs_s < bitmap_s) ? 2 : 1;
+        else if (o->top_counter == 2) top_mode = c->csr_exact ? 2 : 1;
+        else top_mode = (c->csr_exact && pairs_s < bitmap_s) ? 2 : 1;
     }
     const bool top_b1 = o->counter == TFIM_COUNTER_TENSOR || (o->counter != TFIM_COUNTER_LOP3 && n0 >= 16);
 
@@ -1022,6 +1048,9 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
         P.cap_out = cap_out; P.cap_tiles = cap_tiles; P.counter = o->counter; P.la_mode = la_mode;
         P.log_on = o->log_lookahead; P.proposal_threshold = c->proposal_threshold; P.kslice_min = 64; P.sm_count = sm_count;
         P.mlp_w = nullptr; P.mlp_p = nullptr;
+        P.proj_list = (int32_t*)R.proj_list.p;
+        P.avg_len = c->n_bits > 0 ? (float)((double)c->n_red_items / (double)c->n_bits) : 0.f;
+        P.csr_ok = c->csr_exact ? 1 : 0;
         if (la_mode == 2 && c->proposal) {
             const void* wb = nullptr;
             const float* pp = nullptr;
@@ -1163,6 +1192,11 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
             a.tiles = P.tiles_b1;
             a.n_tiles = hst->tiles_b1;
             TFIM_TRY(launch_count_b1(a, s));
+            launches++;
+            count_launches++;
+        }
+        if (hst->n_proj) {
+            TFIM_TRY(launch_count_proj(a, P.proj_list, hst->n_proj, c->d_red_off, c->d_red_items, s));
             launches++;
             count_launches++;
         }

@@ -142,6 +142,10 @@ int launch_count_b1(const CountArgs& a, cudaStream_t s);
 int launch_pair_count(const int64_t* red_off, const int32_t* red_items, int64_t n_red, const int32_t* pos,
                       int32_t nF, int32_t* M, cudaStream_t s);
 int launch_mirror(int32_t* M, int32_t nF, const int32_t* diag, cudaStream_t s);
+// Projected counting of family jobs (count_proj.cu): one block per listed job.
+int launch_count_proj(const CountArgs& a, const int32_t* job_ids, int32_t n_jobs, const int64_t* red_off,
+                      const int32_t* red_items, cudaStream_t s);
+constexpr int kProjMaxCols = 2048;  // longest column list the projected counter hashes
 int launch_materialize(const uint32_t* bitmap, int64_t W, uint32_t* masks, const MatDesc* mats,
                        const int32_t* items, int32_t n, cudaStream_t s);
 // nfreq[g] = #{c < n_cols : counts[g*n_cols + c] >= min_count} for g < n_rows
@@ -180,6 +184,8 @@ struct tfim_ctx {
     int32_t* d_red_items = nullptr;
     int64_t n_red_items = 0;
     double red_pair_work = 0;              // sum over reduced rows of length^2
+    bool csr_exact = false;                // the reduced list repeats no id within a row: the
+                                           // list-based counters (pairs, projected) are exact
     // scratch
     tfim::DevBuf d_scratch[8];
     tfim::HostBuf h_scratch[4];

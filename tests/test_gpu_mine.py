@@ -28,6 +28,8 @@ VARIANTS = [
     dict(engine="resident", counter="tensor", lookahead=True, top="bitmap"),
     dict(engine="resident", counter="auto", lookahead="all", wave_cap=37),
     dict(engine="resident", counter="auto", lookahead=True, top="pairs"),
+    dict(engine="resident", counter="proj", lookahead="learned"),
+    dict(engine="resident", counter="proj", lookahead="all", wave_cap=29),
 ]
 PLAIN_OK = {"cfg1_full", "cfg2_full", "cfg3_base", "cfg3_base_t30", "cfg4_s001", "cfg5_s002", "edge_dups",
             "edge_format", "edge_identical", "edge_item0", "edge_none", "edge_single", "edge_ties"}
