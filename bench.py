@@ -11,8 +11,8 @@ One step = one complete mine of the database (search + every support count), bit
 already resident in HBM.  `value` is throughput in reference-equivalent supports per
 second: the number of supports the reference engine counts for this database (its nodes
 x survivors, measured by the plain engine, which runs the reference's search) divided by
-the batched engine's mine time, summed over ranks (each rank mines its own copy: weak
-scaling).  `e2e` is the same metric through the C ABI from pinned host buffers: build
+the resident batched engine's mine time with the learned lookahead proposal, summed over
+ranks (each rank mines its own copy: weak scaling).  `e2e` is the same metric through the C ABI from pinned host buffers: build
 the device database from the host CSR, mine, read the MFIs back, every step.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl tfim|reference] [--workload cfg4]
@@ -174,7 +174,8 @@ def main() -> int:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="tfim", choices=["tfim", "reference"])
     ap.add_argument("--workload", default="cfg4", choices=sorted(WORKLOADS))
-    ap.add_argument("--counter", default="auto", choices=["auto", "lop3", "tensor"])
+    ap.add_argument("--counter", default="auto", choices=["auto", "lop3", "tensor", "proj"])
+    ap.add_argument("--engine", default="resident", choices=["batched", "resident"])
     ap.add_argument("--lookahead", default="learned", choices=["off", "filtered", "learned", "all"])
     ap.add_argument("--ref-scale", type=float, default=0.02)
     ap.add_argument("--cpu-budget", type=float, default=15.0)
@@ -219,7 +220,7 @@ def main() -> int:
 
     db = tf.Database.from_csr(off_np, items_np, w["minsup"], device=local)
     info = db.info
-    mine_kw = dict(engine="batched", counter=args.counter, lookahead=args.lookahead)
+    mine_kw = dict(engine=args.engine, counter=args.counter, lookahead=args.lookahead)
     for _ in range(args.warmup):
         db.mine(**mine_kw)
     barrier()
@@ -283,7 +284,7 @@ def main() -> int:
                 "traffic": traffic, "bytes_alg_per_launch": tot_bytes / max(1, tot_launch),
                 "kernel_ms_per_launch": tot_kms / max(1, tot_launch),
                 "bitops_per_s": tot_bitops / (tot_kms / 1000.0) if tot_kms > 0 else 0.0,
-                "kernel": "k_count_b1 / k_count_lop3 (counting launches of the batched engine)"}
+                "kernel": "counting launches of the search (k_count_lop3 / k_count_b1 / k_pair_count)"}
 
     # CPU baseline: the oracle port (multithreaded AND+popcount, the reference's search)
     cpu = None
@@ -308,7 +309,7 @@ def main() -> int:
                    "reduced_rows": info["trans_num_reduced"], "survivors": info["n_survivors"],
                    "bitmap_bytes": int(info["n_dense"]) * int(info["words_per_row"]) * 4,
                    "l2": "inputs larger than L2 (bitmap) and a 256 MB L2 flush before every timed step",
-                   "engine": "batched", "counter": args.counter, "lookahead": args.lookahead,
+                   "engine": args.engine, "counter": args.counter, "lookahead": args.lookahead,
                    "parallelism": f"{world} independent database replicas, one per GPU"},
         "mine_time_s": ms / 1000.0,
         "plain_mine_time_s": plain.stats["device_ms"] / 1000.0 if plain else None,

@@ -166,7 +166,9 @@ typedef struct {
     int32_t top_counter;   /* family of the empty prefix: 0 by cost model, 1 bitmap Gram,
                               2 pair co-occurrence over the reduced transaction list */
     int32_t log_lookahead; /* 1: log features and outcomes of every lookahead issued */
-    int32_t reserved[9];
+    int32_t proj_auto;     /* resident engine, automatic counter choice may pick the projected
+                              counter: -1 tuned default, 0 no, 1 yes */
+    int32_t reserved[8];
 } tfim_mine_opts;
 
 typedef struct {

@@ -143,6 +143,7 @@ void tfim_mine_opts_default(tfim_mine_opts* o) {
     o->wave_cap = 0;
     o->lookahead = 1;
     o->use_graphs = 0;
+    o->proj_auto = -1;
 }
 
 }  // extern "C"

@@ -102,6 +102,7 @@ struct ResPtrs {
     int32_t* proj_list;           // family jobs counted by the projected counter
     float avg_len;                // mean reduced transaction length
     int32_t csr_ok;               // the reduced transaction list repeats no id within a row
+    int32_t proj_auto;            // let the automatic counter choice pick the projected counter
 };
 
 // Projected counting pays when the prefix holds few transactions: it walks the base's set
@@ -111,7 +112,7 @@ __device__ __forceinline__ bool use_proj(const ResPtrs& p, const JobDesc& jd, in
     if (!p.csr_ok || jd.n_cols > kProjMaxCols || (jd.base_slot >= 0 && jd.base_item >= 0)) return false;
     if (jd.base_slot < 0 && jd.base_item < 0) return false;
     if (p.counter == TFIM_COUNTER_PROJ) return true;
-    if (p.counter != TFIM_COUNTER_AUTO) return false;
+    if (p.counter != TFIM_COUNTER_AUTO || !p.proj_auto) return false;
     const double proj = (double)p.W + (double)sup * 6.0 * (double)p.avg_len;
     const double bitmap = (double)(jd.n_rows + jd.n_cols + 1) * (double)p.W;
     return proj < bitmap;
@@ -1051,6 +1052,7 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
         P.proj_list = (int32_t*)R.proj_list.p;
         P.avg_len = c->n_bits > 0 ? (float)((double)c->n_red_items / (double)c->n_bits) : 0.f;
         P.csr_ok = c->csr_exact ? 1 : 0;
+        P.proj_auto = o->proj_auto >= 0 ? o->proj_auto : kTuneProjAuto;
         if (la_mode == 2 && c->proposal) {
             const void* wb = nullptr;
             const float* pp = nullptr;

@@ -119,6 +119,7 @@ constexpr double kTuneB1BitOps = 1.9e14;       // b1 tensor-core tiles, bit-ops/
 constexpr double kTuneLop3BitOps = 1.0e14;     // AND+popc tiles, bit-ops/s
 constexpr double kTunePairIncrements = 2.0e10; // pair co-occurrence increments/s
 constexpr double kTuneHbmBytes = 6.5e12;       // bytes/s
+constexpr int kTuneProjAuto = 0;               // projected counter in the automatic choice
 
 constexpr int kLop3Rows = 8;        // rows per CUDA-core tile
 constexpr int kLop3Chunk = 1024;    // max words per CUDA-core tile
@@ -145,7 +146,7 @@ int launch_mirror(int32_t* M, int32_t nF, const int32_t* diag, cudaStream_t s);
 // Projected counting of family jobs (count_proj.cu): one block per listed job.
 int launch_count_proj(const CountArgs& a, const int32_t* job_ids, int32_t n_jobs, const int64_t* red_off,
                       const int32_t* red_items, cudaStream_t s);
-constexpr int kProjMaxCols = 2048;  // longest column list the projected counter hashes
+constexpr int kProjMaxCols = 1024;  // longest column list the projected counter hashes
 int launch_materialize(const uint32_t* bitmap, int64_t W, uint32_t* masks, const MatDesc* mats,
                        const int32_t* items, int32_t n, cudaStream_t s);
 // nfreq[g] = #{c < n_cols : counts[g*n_cols + c] >= min_count} for g < n_rows

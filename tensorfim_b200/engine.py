@@ -157,7 +157,7 @@ class Database:
         return x, y
 
     def mine(self, engine: str = "batched", counter: str = "auto", lookahead=True,
-             wave_cap: int = 0, top: str = "auto", log_lookahead: bool = False) -> MineResult:
+             wave_cap: int = 0, top: str = "auto", log_lookahead: bool = False, proj_auto: int = -1) -> MineResult:
         """lookahead: False/"off", True/"filtered" (every node passing the exact tail-pair
         filter), "learned" (the attached proposal, or the shipped weights), "all"."""
         o = _lib.MineOpts()
@@ -170,6 +170,7 @@ class Database:
             self.set_proposal(Proposal.load(device=self._device))
         o.lookahead = la
         o.log_lookahead = int(log_lookahead)
+        o.proj_auto = int(proj_auto)
         o.wave_cap = int(wave_cap)
         o.top_counter = {"auto": 0, "bitmap": 1, "pairs": 2}[top]
         st = _lib.MineStats()
