@@ -162,13 +162,18 @@ typedef struct {
     int32_t wave_cap;      /* max family rows per wave; 0 = tuned default */
     int32_t lookahead;     /* 0 off, 1 every node that passes the tail-pair filter,
                               2 learned proposal (tfim_set_proposal), 3 every node (no filter) */
-    int32_t use_graphs;    /* replay wave launches as CUDA graphs when possible */
+    int32_t use_graphs;    /* resident engine: run the wave loop as one captured CUDA graph
+                              (conditional WHILE node: pack, count, expand repeat on the
+                              device; the host reads the status when the search ends or a
+                              pool must grow) */
     int32_t top_counter;   /* family of the empty prefix: 0 by cost model, 1 bitmap Gram,
                               2 pair co-occurrence over the reduced transaction list */
     int32_t log_lookahead; /* 1: log features and outcomes of every lookahead issued */
     int32_t proj_auto;     /* resident engine, automatic counter choice may pick the projected
                               counter: -1 tuned default, 0 no, 1 yes */
-    int32_t reserved[8];
+    int32_t small_pools;   /* resident engine: start from minimal pool capacities so that
+                              every pool grows during the search (exercises the growth path) */
+    int32_t reserved[7];
 } tfim_mine_opts;
 
 typedef struct {

@@ -65,8 +65,8 @@ class DbInfo(C.Structure):
 class MineOpts(C.Structure):
     _fields_ = [("engine", C.c_int32), ("counter", C.c_int32), ("wave_cap", C.c_int32),
                 ("lookahead", C.c_int32), ("use_graphs", C.c_int32), ("top_counter", C.c_int32),
-                ("log_lookahead", C.c_int32), ("proj_auto", C.c_int32),
-                ("reserved", C.c_int32 * 8)]
+                ("log_lookahead", C.c_int32), ("proj_auto", C.c_int32), ("small_pools", C.c_int32),
+                ("reserved", C.c_int32 * 7)]
 
 
 class MineStats(C.Structure):

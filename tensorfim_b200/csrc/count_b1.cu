@@ -55,15 +55,19 @@ __device__ __forceinline__ void mma_b1(int32_t (&d)[4], const uint32_t (&a)[4], 
 // byte offset of 16-byte chunk `ch` (0..15) of staged row `row` (0..63), swizzled
 __device__ __forceinline__ uint32_t swz(int row, int ch) { return (uint32_t)(row * kRowBytes + ((ch ^ (row & 7)) << 4)); }
 
-// Block: 256 threads (8 warps as 2 x 4; each warp owns 32 rows x 16 columns).
-__global__ void __launch_bounds__(256) k_count_b1(CountArgs a) {
-    extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ const uint32_t* row_src[64];
-    __shared__ const uint32_t* col_src[64];
-    __shared__ int32_t row_kind[64];   // 0 = source row, 1 = all ones, 2 = zeros
-    __shared__ int32_t col_kind[64];
+struct B1Shared {
+    const uint32_t* row_src[64];
+    const uint32_t* col_src[64];
+    int32_t row_kind[64];   // 0 = source row, 1 = all ones, 2 = zeros
+    int32_t col_kind[64];
+};
 
-    const TileDesc t = a.tiles[blockIdx.x];
+// Block: 256 threads (8 warps as 2 x 4; each warp owns 32 rows x 16 columns).
+__device__ void b1_tile(const CountArgs& a, const TileDesc t, unsigned char* smem, B1Shared& sh) {
+    const uint32_t** row_src = sh.row_src;
+    const uint32_t** col_src = sh.col_src;
+    int32_t* row_kind = sh.row_kind;
+    int32_t* col_kind = sh.col_kind;
     const JobDesc j = a.jobs[t.job];
     const int64_t W = a.W;
     const int tid = threadIdx.x;
@@ -198,20 +202,69 @@ __global__ void __launch_bounds__(256) k_count_b1(CountArgs a) {
                 if (v && r < t.nr && t.c0 + c < t.c1)
                     atomicAdd(a.out + j.out_off + (int64_t)(t.r0 + r) * j.n_cols + (t.c0 + c), v);
             }
+    __syncthreads();   // the block's next tile reuses the staging and the source tables
+}
+
+__global__ void __launch_bounds__(256) k_count_b1(CountArgs a) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ B1Shared sh;
+    b1_tile(a, a.tiles[blockIdx.x], smem, sh);
+}
+
+__global__ void __launch_bounds__(256) k_count_b1_persistent(const CountArgs* __restrict__ args, const int32_t* n_tiles) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ B1Shared sh;
+    const CountArgs a = *args;
+    const int32_t n = *n_tiles;
+    for (int32_t t = blockIdx.x; t < n; t += gridDim.x) b1_tile(a, a.tiles[t], smem, sh);
 }
 
 }  // namespace
 
+int configure_count_kernels() {
+    // dynamic shared memory above 48 KiB is opted into once per device
+    static bool done[64] = {};
+    int dev = 0;
+    TFIM_CUDA(cudaGetDevice(&dev));
+    if (dev >= 0 && dev < 64 && done[dev]) return TFIM_OK;
+    const size_t smem = (size_t)kStages * kStageBytes;
+    TFIM_CUDA(cudaFuncSetAttribute(k_count_b1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    TFIM_CUDA(cudaFuncSetAttribute(k_count_b1_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (dev >= 0 && dev < 64) done[dev] = true;
+    return TFIM_OK;
+}
+
 int launch_count_b1(const CountArgs& a, cudaStream_t s) {
     if (a.n_tiles <= 0) return TFIM_OK;
+    TFIM_TRY(configure_count_kernels());
     const size_t smem = (size_t)kStages * kStageBytes;
-    static bool configured = false;
-    if (!configured) {
-        TFIM_CUDA(cudaFuncSetAttribute(k_count_b1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        configured = true;
-    }
     k_count_b1<<<a.n_tiles, 256, smem, s>>>(a);
     TFIM_CUDA(cudaGetLastError());
+    return TFIM_OK;
+}
+
+int occupancy_b1(int* blocks) {
+    TFIM_TRY(configure_count_kernels());
+    TFIM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, k_count_b1_persistent, 256,
+                                                             (size_t)kStages * kStageBytes));
+    return TFIM_OK;
+}
+
+int launch_count_b1_persistent(const CountArgs* d_args, const int32_t* d_n_tiles, int32_t grid, cudaStream_t s) {
+    TFIM_TRY(configure_count_kernels());
+    const size_t smem = (size_t)kStages * kStageBytes;
+    k_count_b1_persistent<<<grid, 256, smem, s>>>(d_args, d_n_tiles);
+    TFIM_CUDA(cudaGetLastError());
+    return TFIM_OK;
+}
+
+int occupancy_lop3(int* blocks);
+int occupancy_proj(int* blocks);
+
+int persistent_occupancy(int* lop3, int* b1, int* proj) {
+    TFIM_TRY(occupancy_lop3(lop3));
+    TFIM_TRY(occupancy_b1(b1));
+    TFIM_TRY(occupancy_proj(proj));
     return TFIM_OK;
 }
 

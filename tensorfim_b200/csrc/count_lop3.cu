@@ -15,63 +15,178 @@ namespace {
 __device__ __forceinline__ uint4 and4(uint4 a, uint4 b) { return make_uint4(a.x & b.x, a.y & b.y, a.z & b.z, a.w & b.w); }
 __device__ __forceinline__ uint32_t popc4(uint4 a) { return __popc(a.x) + __popc(a.y) + __popc(a.z) + __popc(a.w); }
 
-// Block: 256 threads.  Shared memory: kLop3Rows x kLop3Chunk words.  A tile may span
-// any word range; it is processed kLop3Chunk words at a time.
-__global__ void __launch_bounds__(256) k_count_lop3(CountArgs a) {
-    extern __shared__ uint4 sm4[];
-    __shared__ const uint4* rsrc[kLop3Rows][2];
-    const TileDesc t = a.tiles[blockIdx.x];
+// A tile is rows [r0, r0+nr) x columns [c0, c1) of one job over a word range.  Most of a
+// prefix mask is zero, and the jobs of a sparse database are narrow (a few rows and
+// columns), so the tile neither streams whole rows nor gives each column a warp.  Every
+// warp works on its own 128-position (2048-bit) stripes, without block barriers:
+//   (1) candidates: each lane tests 4 consecutive 128-bit positions of the base mask;
+//   (2) rounds: each lane takes its next candidate, loads the tile's rows there and keeps
+//       the position when any row survives the base; kept positions are compacted by
+//       ballot into the warp's staging region with the masked row values;
+//   (3) flush: lanes are spread over (staged position, column) pairs -- 32 / ncols
+//       positions per pass -- gather the column words and accumulate
+//       popc(staged row & column) in registers for the whole word range.
+// The warps' partial sums meet in shared memory and one global atomic per (row, column)
+// is issued per tile.  Row words are read only where the base is nonzero, column words
+// only where a row of the tile survives.
+constexpr int kL3Stage = 2048;   // staged 128-bit values (positions x rows), 32 KiB, 1/8 per warp
+constexpr int kL3Pos = 1024;     // staged positions, 1/8 per warp
+constexpr int kL3Step = 1024;    // positions per step (128 per warp, 4 per lane)
+
+struct Lop3Shared {
+    uint4 staged[kL3Stage];
+    int32_t pos[kL3Pos];
+    int32_t acc[kLop3Rows * 64];
+    const uint4* rsrc[kLop3Rows][2];
+};
+
+__device__ __forceinline__ bool nonzero4(uint4 v) { return (v.x | v.y | v.z | v.w) != 0u; }
+
+__device__ void lop3_tile(const CountArgs& a, const TileDesc t, Lop3Shared& sh) {
     const JobDesc j = a.jobs[t.job];
     const int64_t W = a.W;
-    if (threadIdx.x < kLop3Rows && (int)threadIdx.x < t.nr) {
-        const RowDesc rd = a.rows[j.row_off + t.r0 + threadIdx.x];
-        rsrc[threadIdx.x][0] = rd.slot >= 0 ? reinterpret_cast<const uint4*>(a.masks + (int64_t)rd.slot * W) : nullptr;
-        rsrc[threadIdx.x][1] = rd.item >= 0 ? reinterpret_cast<const uint4*>(a.bitmap + (int64_t)rd.item * W) : nullptr;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nr = t.nr;
+    const int ncols = t.c1 - t.c0;
+    if (tid < kLop3Rows && tid < nr) {
+        const RowDesc rd = a.rows[j.row_off + t.r0 + tid];
+        sh.rsrc[tid][0] = rd.slot >= 0 ? reinterpret_cast<const uint4*>(a.masks + (int64_t)rd.slot * W) : nullptr;
+        sh.rsrc[tid][1] = rd.item >= 0 ? reinterpret_cast<const uint4*>(a.bitmap + (int64_t)rd.item * W) : nullptr;
     }
+    for (int q = tid; q < kLop3Rows * 64; q += blockDim.x) sh.acc[q] = 0;
     const uint4* base_m = j.base_slot >= 0 ? reinterpret_cast<const uint4*>(a.masks + (int64_t)j.base_slot * W) : nullptr;
     const uint4* base_i = j.base_item >= 0 ? reinterpret_cast<const uint4*>(a.bitmap + (int64_t)j.base_item * W) : nullptr;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int cw = t.w0; cw < t.w1; cw += kLop3Chunk) {
-        const int w4b = cw >> 2;
-        const int nw4 = (min(t.w1, cw + kLop3Chunk) - cw) >> 2;
-        __syncthreads();   // rsrc visible; previous chunk's readers done
-        // 1. stage the tile's row masks for this word chunk
-        for (int r = 0; r < t.nr; r++) {
-            const uint4* rs = rsrc[r][0];
-            const uint4* ri = rsrc[r][1];
-            for (int w = threadIdx.x; w < nw4; w += blockDim.x) {
-                uint4 m = make_uint4(~0u, ~0u, ~0u, ~0u);
-                if (base_m) m = and4(m, __ldg(base_m + w4b + w));
-                if (base_i) m = and4(m, __ldg(base_i + w4b + w));
-                if (rs) m = and4(m, __ldg(rs + w4b + w));
-                if (ri) m = and4(m, __ldg(ri + w4b + w));
-                sm4[r * nw4 + w] = m;
-            }
-        }
-        __syncthreads();
-        // 2. one warp per column: stream the column row through every staged row
-        for (int c = t.c0 + warp; c < t.c1; c += 8) {
-            const int32_t col = c == j.self_col ? -1 : a.cols[j.col_off + c];
-            const uint4* cp = col >= 0 ? reinterpret_cast<const uint4*>(a.bitmap + (int64_t)col * W) + w4b : nullptr;
-            uint32_t acc[kLop3Rows];
+    // flush layout: G staged positions per pass, lane -> (position offset, column(s))
+    const bool wide = ncols > 32;
+    const int G = wide ? 1 : 32 / ncols;
+    const int koff = wide ? 0 : lane / ncols;
+    const bool active = koff < G;
+    const int cl[2] = {wide ? lane : lane % ncols, wide ? lane + 32 : -1};
+    const uint4* cp[2];
+    int ck[2];   // 0: column row, 1: all ones, 2: none
 #pragma unroll
-            for (int r = 0; r < kLop3Rows; r++) acc[r] = 0;
-            for (int w = lane; w < nw4; w += 32) {
-                const uint4 v = cp ? __ldg(cp + w) : make_uint4(~0u, ~0u, ~0u, ~0u);
-#pragma unroll
-                for (int r = 0; r < kLop3Rows; r++)
-                    if (r < t.nr) acc[r] += popc4(and4(sm4[r * nw4 + w], v));
-            }
-#pragma unroll
-            for (int r = 0; r < kLop3Rows; r++) {
-                if (r >= t.nr) break;
-                uint32_t v = acc[r];
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-                if (lane == 0 && v) atomicAdd(a.out + j.out_off + (int64_t)(t.r0 + r) * j.n_cols + c, (int32_t)v);
+    for (int ci = 0; ci < 2; ci++) {
+        const int c = t.c0 + cl[ci];
+        ck[ci] = 2;
+        cp[ci] = nullptr;
+        if (cl[ci] >= 0 && cl[ci] < ncols && active) {
+            if (c == j.self_col) ck[ci] = 1;
+            else {
+                ck[ci] = 0;
+                cp[ci] = reinterpret_cast<const uint4*>(a.bitmap + (int64_t)a.cols[j.col_off + c] * W);
             }
         }
     }
+    uint32_t acc[2][kLop3Rows];
+#pragma unroll
+    for (int ci = 0; ci < 2; ci++)
+#pragma unroll
+        for (int r = 0; r < kLop3Rows; r++) acc[ci][r] = 0;
+    __syncthreads();   // rsrc, acc
+    uint4* wst = sh.staged + warp * (kL3Stage / 8);
+    int32_t* wpos = sh.pos + warp * (kL3Pos / 8);
+    const int wcap = min(kL3Pos / 8, (kL3Stage / 8) / nr);
+    int ns = 0;   // staged positions of this warp (warp-uniform)
+
+    auto flush = [&]() {
+        __syncwarp();
+        for (int k0 = 0; k0 < ns; k0 += G) {
+            const int k = k0 + koff;
+            if (!active || k >= ns) continue;
+            const int p = wpos[k];
+            uint4 v[2];
+#pragma unroll
+            for (int ci = 0; ci < 2; ci++)
+                v[ci] = ck[ci] == 0 ? __ldg(cp[ci] + p) : ck[ci] == 1 ? make_uint4(~0u, ~0u, ~0u, ~0u) : make_uint4(0, 0, 0, 0);
+            const uint4* st = wst + k * nr;
+#pragma unroll
+            for (int r = 0; r < kLop3Rows; r++) {
+                if (r >= nr) break;
+                const uint4 m = st[r];
+                acc[0][r] += popc4(and4(m, v[0]));
+                if (wide) acc[1][r] += popc4(and4(m, v[1]));
+            }
+        }
+        __syncwarp();
+        ns = 0;
+    };
+    auto base_at = [&](int64_t p) {
+        uint4 x = make_uint4(~0u, ~0u, ~0u, ~0u);
+        if (base_m) x = and4(x, __ldg(base_m + p));
+        if (base_i) x = and4(x, __ldg(base_i + p));
+        return x;
+    };
+    auto row_at = [&](int r, uint4 x, int64_t p) {
+        const uint4* rs = sh.rsrc[r][0];
+        const uint4* ri = sh.rsrc[r][1];
+        if (rs) x = and4(x, __ldg(rs + p));
+        if (ri) x = and4(x, __ldg(ri + p));
+        return x;
+    };
+
+    const int64_t P0 = t.w0 >> 2, P1 = t.w1 >> 2;
+    const unsigned lt = (1u << lane) - 1u;
+    for (int64_t s0 = P0 + warp * 128; s0 < P1; s0 += kL3Step) {
+        // (1) candidates: nonzero base positions, 4 consecutive per lane
+        const int64_t pl = s0 + 4 * lane;
+        uint32_t valid = 0;
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+            if (pl + q < P1 && nonzero4(base_at(pl + q))) valid |= 1u << q;
+        // (2) rounds: each lane its next candidate.  The row words are read twice (to test,
+        // then to stage); the second read hits L1.
+        while (__any_sync(0xffffffffu, valid != 0)) {
+            const int q_sel = valid ? __ffs(valid) - 1 : -1;
+            valid &= valid - 1;
+            const int64_t p = pl + q_sel;
+            bool any = false;
+            uint4 b = make_uint4(0, 0, 0, 0);
+            if (q_sel >= 0) {
+                b = base_at(p);
+#pragma unroll
+                for (int r = 0; r < kLop3Rows; r++)
+                    if (r < nr) any |= nonzero4(row_at(r, b, p));
+            }
+            if (ns + 32 > wcap) flush();
+            const unsigned bal = __ballot_sync(0xffffffffu, any);
+            if (any) {
+                const int k = ns + __popc(bal & lt);
+                wpos[k] = (int32_t)p;
+#pragma unroll
+                for (int r = 0; r < kLop3Rows; r++)
+                    if (r < nr) wst[k * nr + r] = row_at(r, b, p);
+            }
+            ns += __popc(bal);
+        }
+    }
+    if (ns > 0) flush();
+    // partial sums of the warps meet in shared memory; one global atomic per output
+#pragma unroll
+    for (int ci = 0; ci < 2; ci++)
+#pragma unroll
+        for (int r = 0; r < kLop3Rows; r++)
+            if (r < nr && ck[ci] != 2 && acc[ci][r]) atomicAdd(&sh.acc[r * 64 + cl[ci]], (int32_t)acc[ci][r]);
+    __syncthreads();
+    for (int q = tid; q < nr * ncols; q += blockDim.x) {
+        const int r = q / ncols, c = q - r * ncols;
+        const int32_t v = sh.acc[r * 64 + c];
+        if (v) atomicAdd(a.out + j.out_off + (int64_t)(t.r0 + r) * j.n_cols + t.c0 + c, v);
+    }
+    __syncthreads();   // shared state is reused by the block's next tile
+}
+
+__global__ void __launch_bounds__(256, 4) k_count_lop3(CountArgs a) {
+    __shared__ Lop3Shared sh;
+    lop3_tile(a, a.tiles[blockIdx.x], sh);
+}
+
+// Persistent form: arguments and tile count are read from device memory (a wave built on the GPU).
+__global__ void __launch_bounds__(256, 4) k_count_lop3_persistent(const CountArgs* __restrict__ args,
+                                                               const int32_t* n_tiles) {
+    __shared__ Lop3Shared sh;
+    const CountArgs a = *args;
+    const int32_t n = *n_tiles;
+    for (int32_t t = blockIdx.x; t < n; t += gridDim.x) lop3_tile(a, a.tiles[t], sh);
 }
 
 // masks[dst] = (src >= 0 ? masks[src] : ~0) & AND of the listed item rows.
@@ -143,13 +258,18 @@ __global__ void k_compact(const int32_t* __restrict__ counts, const JobDesc* __r
 
 int launch_count_lop3(const CountArgs& a, cudaStream_t s) {
     if (a.n_tiles <= 0) return TFIM_OK;
-    const size_t smem = (size_t)kLop3Rows * kLop3Chunk * 4;
-    static bool configured = false;
-    if (!configured) {
-        TFIM_CUDA(cudaFuncSetAttribute(k_count_lop3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        configured = true;
-    }
-    k_count_lop3<<<a.n_tiles, 256, smem, s>>>(a);
+    k_count_lop3<<<a.n_tiles, 256, 0, s>>>(a);
+    TFIM_CUDA(cudaGetLastError());
+    return TFIM_OK;
+}
+
+int occupancy_lop3(int* blocks) {
+    TFIM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, k_count_lop3_persistent, 256, 0));
+    return TFIM_OK;
+}
+
+int launch_count_lop3_persistent(const CountArgs* d_args, const int32_t* d_n_tiles, int32_t grid, cudaStream_t s) {
+    k_count_lop3_persistent<<<grid, 256, 0, s>>>(d_args, d_n_tiles);
     TFIM_CUDA(cudaGetLastError());
     return TFIM_OK;
 }

@@ -75,14 +75,19 @@ __device__ void thread_transaction(int64_t r, const int64_t* __restrict__ red_of
     }
 }
 
-__global__ void __launch_bounds__(kProjWarps * 32) k_count_proj(CountArgs a, const int32_t* __restrict__ job_ids,
-                                                                const int64_t* __restrict__ red_off,
-                                                                const int32_t* __restrict__ red_items) {
-    __shared__ int32_t keys[kProjHash];
-    __shared__ int32_t vals[kProjHash];
-    __shared__ int32_t acc[kProjAcc];
-    __shared__ int32_t tidbuf[kProjWarps][kProjTidBuf];
-    const int32_t jid = job_ids[blockIdx.x];
+struct ProjShared {
+    int32_t keys[kProjHash];
+    int32_t vals[kProjHash];
+    int32_t acc[kProjAcc];
+    int32_t tidbuf[kProjWarps][kProjTidBuf];
+};
+
+__device__ void proj_job(const CountArgs& a, int32_t jid, const int64_t* __restrict__ red_off,
+                         const int32_t* __restrict__ red_items, ProjShared& sh) {
+    int32_t* keys = sh.keys;
+    int32_t* vals = sh.vals;
+    int32_t* acc = sh.acc;
+    int32_t (*tidbuf)[kProjTidBuf] = sh.tidbuf;
     const JobDesc j = a.jobs[jid];
     const int nr = j.n_rows, nc = j.n_cols;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -161,9 +166,39 @@ __global__ void __launch_bounds__(kProjWarps * 32) k_count_proj(CountArgs a, con
     __syncthreads();
     if (smem_acc)
         for (int q = threadIdx.x; q < nr * nc; q += blockDim.x) out[q] = acc[q];
+    __syncthreads();   // the block's next job reuses the tables
+}
+
+__global__ void __launch_bounds__(kProjWarps * 32) k_count_proj(CountArgs a, const int32_t* __restrict__ job_ids,
+                                                                const int64_t* __restrict__ red_off,
+                                                                const int32_t* __restrict__ red_items) {
+    __shared__ ProjShared sh;
+    proj_job(a, job_ids[blockIdx.x], red_off, red_items, sh);
+}
+
+__global__ void __launch_bounds__(kProjWarps * 32) k_count_proj_persistent(const CountArgs* __restrict__ args,
+                                                                           const int32_t* n_jobs,
+                                                                           const int64_t* __restrict__ red_off,
+                                                                           const int32_t* __restrict__ red_items) {
+    __shared__ ProjShared sh;
+    const CountArgs a = *args;
+    const int32_t n = *n_jobs;
+    for (int32_t q = blockIdx.x; q < n; q += gridDim.x) proj_job(a, a.job_list[q], red_off, red_items, sh);
 }
 
 }  // namespace
+
+int occupancy_proj(int* blocks) {
+    TFIM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, k_count_proj_persistent, kProjWarps * 32, 0));
+    return TFIM_OK;
+}
+
+int launch_count_proj_persistent(const CountArgs* d_args, const int32_t* d_n_jobs, int32_t grid, const int64_t* red_off,
+                                 const int32_t* red_items, cudaStream_t s) {
+    k_count_proj_persistent<<<grid, kProjWarps * 32, 0, s>>>(d_args, d_n_jobs, red_off, red_items);
+    TFIM_CUDA(cudaGetLastError());
+    return TFIM_OK;
+}
 
 int launch_count_proj(const CountArgs& a, const int32_t* job_ids, int32_t n_jobs, const int64_t* red_off,
                       const int32_t* red_items, cudaStream_t s) {

@@ -54,8 +54,27 @@ struct ResStatus {
     int32_t jobs, rows, tiles_l3, tiles_b1, n_proj, pad0;
     int64_t out_total;
     int32_t max_cols, max_head, starved, error;
-    unsigned long long supports, nodes, lookaheads, hits, skipped, pep;
+    // grow: the wave the pack built does not fit the pools; nothing was consumed and the
+    // g_* fields hold its size, for the host to grow the pools and pack again
+    int32_t grow, g_rows, g_jobs, g_max_head, g_max_cols, waves;
+    int64_t g_out, g_tiles;
+    int32_t launch_id, pad1;
+    unsigned long long launch_t0, count_t0;
+    unsigned long long supports, nodes, lookaheads, hits, skipped, pep, bytes_alg, count_ns;
 };
+
+// Pool capacities, in entries.  A wave is packed only when the worst case of its expand fits.
+struct Caps {
+    int64_t fam, item, head, mfi, mfi_items, looks, slots, log, rows;
+};
+__host__ __device__ __forceinline__ bool wave_fits(const Caps& c, const ResStatus& st, int64_t rows, int64_t jobs,
+                                                   int64_t out_total, int64_t max_head, int64_t max_cols, bool log_on) {
+    const int64_t list = max_head + 2 + max_cols;
+    return st.fam_n + rows + 1 <= c.fam && st.item_n + 2 * out_total + rows + 1 <= c.item &&
+           st.head_n + rows * list + 1 <= c.head && st.mfi_n + rows + jobs + 1 <= c.mfi &&
+           st.mfi_item_n + (rows + jobs) * list + 1 <= c.mfi_items && rows + 1 <= c.looks &&
+           st.slot_n + 2 * rows + 2 <= c.slots && (!log_on || st.log_n + rows + 1 <= c.log) && rows <= c.rows;
+}
 
 struct ResPtrs {
     // pools
@@ -103,7 +122,25 @@ struct ResPtrs {
     float avg_len;                // mean reduced transaction length
     int32_t csr_ok;               // the reduced transaction list repeats no id within a row
     int32_t proj_auto;            // let the automatic counter choice pick the projected counter
+    Caps caps;
+    int64_t row_bytes;            // bytes of one bitmap row (algorithmic traffic accounting)
+    // graph-driven wave loop: stop after wave_limit waves or max_launch_ns of device time
+    int32_t wave_limit, launch_id;
+    unsigned long long max_launch_ns;
 };
+
+// Arguments of the graph-driven wave loop, kept in device memory so that growing a pool
+// only rewrites this record (the captured launches stay valid).
+struct ResArgs {
+    ResPtrs p;
+    CountArgs a3, a1;
+};
+
+__device__ __forceinline__ unsigned long long globaltimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
 
 // Projected counting pays when the prefix holds few transactions: it walks the base's set
 // bits (W words) and looks up about 6 entries per item of each of its sup transactions,
@@ -158,7 +195,7 @@ __device__ __forceinline__ int find_job_by_tile(const DJob* dj, int nj, int64_t 
     return lo;
 }
 
-__global__ void __launch_bounds__(kPackThreads) k_res_pack(ResPtrs p) {
+__device__ __forceinline__ void res_pack(const ResPtrs& p) {
     typedef cub::BlockScan<int64_t, kPackThreads> Scan;
     typedef cub::BlockReduce<int64_t, kPackThreads> Red;
     __shared__ union {
@@ -166,7 +203,7 @@ __global__ void __launch_bounds__(kPackThreads) k_res_pack(ResPtrs p) {
         typename Red::TempStorage red;
     } tmp;
     __shared__ int32_t s_fam[kPackCand];
-    __shared__ int32_t s_n_jobs, s_rows_total, s_done, s_max_cols, s_max_head, s_stack_after, s_kstop;
+    __shared__ int32_t s_n_jobs, s_rows_total, s_done, s_max_cols, s_max_head, s_stack_after, s_kstop, s_fit;
     __shared__ int64_t s_out_total, s_agg;
     ResStatus* st = p.st;
     const int tid = threadIdx.x;
@@ -178,6 +215,12 @@ __global__ void __launch_bounds__(kPackThreads) k_res_pack(ResPtrs p) {
         s_n_jobs = 0; s_rows_total = 0; s_out_total = 0; s_max_cols = 0; s_max_head = 0; s_done = 0;
         s_stack_after = st->stack_n;
         st->n_proj = 0;
+        st->grow = 0;
+        st->starved = 0;
+        if (st->launch_id != p.launch_id) {
+            st->launch_id = p.launch_id;
+            st->launch_t0 = globaltimer();
+        }
     }
     __syncthreads();
     if (tid == 0) {
@@ -226,7 +269,6 @@ __global__ void __launch_bounds__(kPackThreads) k_res_pack(ResPtrs p) {
     if (tid == 0) {
         s_rows_total = n_look;
         s_n_jobs = n_look;
-        st->look_n = 0;
     }
     __syncthreads();
     // (2) families from the top of the stack
@@ -323,7 +365,7 @@ __global__ void __launch_bounds__(kPackThreads) k_res_pack(ResPtrs p) {
             jd.out_off = s_out_total + (oc[q] - ov[q]);
             jd.self_col = -1; jd.pad = 0;
             p.jobs[jid] = jd;
-            fp->next_row = f.next_row + take[q];
+            (void)fp;   // next_row advances when the wave is committed
         }
         __syncthreads();
         // outputs of this pass: every job's taken rows x its columns
@@ -403,7 +445,33 @@ __global__ void __launch_bounds__(kPackThreads) k_res_pack(ResPtrs p) {
     if (wslice <= 0) wslice = 64;
     const int64_t nk = W > 0 ? (W + kslice - 1) / kslice : 1, nw = W > 0 ? (W + wslice - 1) / wslice : 1;
     const int64_t T3 = tot3 * nw, T1 = tot1 * nk;
+    // the wave is committed only when the worst case of its expand fits the pools
+    if (tid == 0) {
+        const bool fit = s_out_total <= p.cap_out && T1 <= p.cap_tiles && T3 <= p.cap_tiles &&
+                         wave_fits(p.caps, *st, rows_total, nj, s_out_total, s_max_head, s_max_cols, p.log_on != 0);
+        s_fit = fit;
+        if (!fit) {
+            st->grow = 1;
+            st->g_rows = rows_total;
+            st->g_jobs = nj;
+            st->g_out = s_out_total;
+            st->g_max_head = s_max_head;
+            st->g_max_cols = s_max_cols;
+            st->g_tiles = lmax(T1, T3);
+        }
+    }
     __syncthreads();
+    if (!s_fit) {
+        if (tid == 0) {
+            st->jobs = 0; st->rows = 0; st->tiles_l3 = 0; st->tiles_b1 = 0; st->n_proj = 0; st->out_total = 0;
+        }
+        return;
+    }
+    // commit: the families hand out their rows
+    for (int j = n_look + tid; j < nj; j += kPackThreads) {
+        const DJob dj = p.djobs[j];
+        p.fams[dj.fam].next_row = dj.r0 + dj.nr;
+    }
     if (T3 <= p.cap_tiles)
         for (int64_t t = tid; t < T3; t += kPackThreads) {
             const int64_t slice = t / tot3, local = t % tot3;
@@ -429,7 +497,6 @@ __global__ void __launch_bounds__(kPackThreads) k_res_pack(ResPtrs p) {
                                      min(jd.n_cols, cc * kB1Cols + kB1Cols), (int32_t)w0, (int32_t)lmin(W, w0 + kslice), 0};
         }
     if (tid == 0) {
-        if (T1 > p.cap_tiles || T3 > p.cap_tiles) st->error = 2;   // tile capacity exceeded
         st->jobs = nj;
         st->rows = rows_total;
         st->tiles_l3 = (int32_t)T3;
@@ -438,9 +505,17 @@ __global__ void __launch_bounds__(kPackThreads) k_res_pack(ResPtrs p) {
         st->max_cols = s_max_cols;
         st->max_head = s_max_head;
         st->stack_n = s_stack_after;
+        st->look_n = 0;
         st->nodes += rows_total;
         st->supports += s_out_total;
+        st->bytes_alg += (unsigned long long)(p.row_bytes * (2LL * rows_total + nj) + 4 * s_out_total);
     }
+}
+
+__global__ void __launch_bounds__(kPackThreads) k_res_pack(ResPtrs p) { res_pack(p); }
+__global__ void __launch_bounds__(kPackThreads) k_res_pack_g(const ResArgs* __restrict__ args) {
+    const ResPtrs p = args->p;
+    res_pack(p);
 }
 
 // ---------------------------------------------------------------------------------- expand helpers
@@ -541,11 +616,8 @@ __device__ float warp_mlp(const ResPtrs& p, float x, int lane) {
 
 // ---------------------------------------------------------------------------------- expand
 // One warp per counted row of the wave.
-__global__ void __launch_bounds__(256) k_res_expand(ResPtrs p) {
-    const int64_t g = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
+__device__ void expand_row(const ResPtrs& p, int64_t g, int lane) {
     ResStatus* st = p.st;
-    if (g >= st->rows) return;
     const int32_t jid = p.row_job[g];
     const int32_t r = p.row_local[g];
     const DJob dj = p.djobs[jid];
@@ -616,21 +688,37 @@ __global__ void __launch_bounds__(256) k_res_expand(ResPtrs p) {
         finish_row(p, fp, lane);
         return;
     }
-    // scan the row: extensions, equal-support items, tail
+    // scan the row: extensions, equal-support items, tail.  Four loads in flight per lane;
+    // `blocks` marks the column blocks of `bs` columns that hold an extension, so that the
+    // later passes read only those.
     bool prune = false;
     int n_ext = 0, n_eq = 0, n_tail = 0;
-    for (int c0 = 0; c0 < nF; c0 += 32) {
-        const int c = c0 + lane;
-        const int32_t v = c < nF && c != i ? crow[c] : -1;
-        const bool e = v >= minc;
-        const bool in_tail = c > i && c < nT;
-        const bool eq = e && v == supc;
-        prune |= eq && !in_tail;
-        n_ext += __popc(__ballot_sync(0xffffffffu, e));
-        n_eq += __popc(__ballot_sync(0xffffffffu, eq));
-        n_tail += __popc(__ballot_sync(0xffffffffu, e && !eq && in_tail));
+    const int bs = max(128, (((nF + 63) >> 6) + 31) & ~31);   // nF / bs <= 64, a multiple of 32
+    unsigned long long blocks = 0;
+    for (int c0 = 0; c0 < nF; c0 += 128) {
+        int32_t v4[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int c = c0 + 32 * u + lane;
+            v4[u] = c < nF && c != i ? crow[c] : -1;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int c = c0 + 32 * u + lane;
+            const int32_t v = v4[u];
+            const bool e = v >= minc;
+            const bool in_tail = c > i && c < nT;
+            const bool eq = e && v == supc;
+            prune |= eq && !in_tail;
+            if (e) blocks |= 1ull << (c / bs);
+            n_ext += __popc(__ballot_sync(0xffffffffu, e));
+            n_eq += __popc(__ballot_sync(0xffffffffu, eq));
+            n_tail += __popc(__ballot_sync(0xffffffffu, e && !eq && in_tail));
+        }
     }
     prune = __any_sync(0xffffffffu, prune);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) blocks |= __shfl_xor_sync(0xffffffffu, blocks, o);
     if (prune) {
         if (lane == 0) atomicAdd(&st->pep, 1ull);
         finish_row(p, fp, lane);
@@ -647,13 +735,16 @@ __global__ void __launch_bounds__(256) k_res_expand(ResPtrs p) {
             eoff = __shfl_sync(0xffffffffu, eoff, 0);
             int32_t* ecols = p.items + eoff;
             int pos = 0;
-            for (int c0 = 0; c0 < nF && n_eq; c0 += 32) {
-                const int c = c0 + lane;
-                const int32_t v = c < nF && c != i ? crow[c] : -1;
-                const bool eq = v >= minc && v == supc;
-                const unsigned bal = __ballot_sync(0xffffffffu, eq);
-                if (eq) ecols[pos + __popc(bal & ((1u << lane) - 1u))] = c;
-                pos += __popc(bal);
+            for (unsigned long long bm = n_eq ? blocks : 0ull; bm; bm &= bm - 1) {
+                const int b0 = (__ffsll((long long)bm) - 1) * bs;
+                for (int c0 = b0; c0 < min(nF, b0 + bs); c0 += 32) {
+                    const int c = c0 + lane;
+                    const int32_t v = c < nF && c != i ? crow[c] : -1;
+                    const bool eq = v >= minc && v == supc;
+                    const unsigned bal = __ballot_sync(0xffffffffu, eq);
+                    if (eq) ecols[pos + __popc(bal & ((1u << lane) - 1u))] = c;
+                    pos += __popc(bal);
+                }
             }
             __syncwarp();
             warp_emit_mfi(p, head, f.head_len, t, ecols, n_eq, F, supc, lane);
@@ -677,9 +768,10 @@ __global__ void __launch_bounds__(256) k_res_expand(ResPtrs p) {
     int32_t* hc = p.heads + hoff;
     for (int q = lane; q < f.head_len; q += 32) hc[q] = head[q];
     if (lane == 0) hc[f.head_len] = t;
-    {
-        int pos_eq = 0, pos_tail = 0, pos_rest = 0;
-        for (int c0 = 0; c0 < nF; c0 += 32) {
+    int pos_eq = 0, pos_tail = 0, pos_rest = 0;
+    for (unsigned long long bm = blocks; bm; bm &= bm - 1) {
+        const int b0 = (__ffsll((long long)bm) - 1) * bs;
+        for (int c0 = b0; c0 < min(nF, b0 + bs); c0 += 32) {
             const int c = c0 + lane;
             const int32_t v = c < nF && c != i ? crow[c] : -1;
             const bool e = v >= minc;
@@ -859,15 +951,62 @@ __global__ void __launch_bounds__(256) k_res_expand(ResPtrs p) {
     finish_row(p, fp, lane);
 }
 
+__global__ void __launch_bounds__(256) k_res_expand(ResPtrs p) {
+    const int64_t g = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    if (g >= p.st->rows) return;
+    expand_row(p, g, threadIdx.x & 31);
+}
+
+// ---------------------------------------------------------------------------------- graph loop
+// The wave loop as a graph: a conditional WHILE node whose body is
+//   pack -> zero the count block -> persistent counters -> persistent expand -> control.
+// Every kernel reads its arguments from the ResArgs record and its sizes from the status
+// record, so the launch shapes are fixed.  The control kernel ends the loop when the search
+// is done, when the pack asks for larger pools or reports an error, or after the slice's
+// wave / time limit; the host then reads the status once.
+
+// Zero the wave's count block; stamps the start of counting.
+__global__ void __launch_bounds__(256) k_res_zero(const ResArgs* __restrict__ args) {
+    ResStatus* st = args->p.st;
+    int32_t* counts = args->p.counts;
+    if (blockIdx.x == 0 && threadIdx.x == 0) st->count_t0 = globaltimer();
+    const int64_t n = st->out_total;
+    const int64_t n4 = n >> 2;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t i0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int4* c4 = reinterpret_cast<int4*>(counts);
+    for (int64_t i = i0; i < n4; i += stride) c4[i] = make_int4(0, 0, 0, 0);
+    for (int64_t i = (n4 << 2) + i0; i < n; i += stride) counts[i] = 0;
+}
+
+__global__ void __launch_bounds__(256) k_res_expand_g(const ResArgs* __restrict__ args) {
+    const ResPtrs p = args->p;
+    const int lane = threadIdx.x & 31;
+    const int32_t rows = p.st->rows;
+    if (blockIdx.x == 0 && threadIdx.x == 0 && rows > 0) p.st->count_ns += globaltimer() - p.st->count_t0;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t g = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; g < rows; g += warps) expand_row(p, g, lane);
+}
+
+__global__ void k_res_control(const ResArgs* __restrict__ args, cudaGraphConditionalHandle h) {
+    if (threadIdx.x != 0) return;
+    ResStatus* st = args->p.st;
+    const bool progressed = st->jobs > 0;
+    if (progressed) st->waves += 1;
+    const bool go = progressed && !st->error && !st->grow && !st->starved && st->waves < args->p.wave_limit &&
+                    globaltimer() - st->launch_t0 < args->p.max_launch_ns;
+    cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+
 // ---------------------------------------------------------------------------------- host
 struct Pool {
     void* p = nullptr;
     size_t bytes = 0;
 };
 
-int grow(Pool& b, size_t need, cudaStream_t s) {
+int grow(Pool& b, size_t need, cudaStream_t s, size_t min_bytes = 1 << 16) {
     if (need <= b.bytes && b.p) return TFIM_OK;
-    size_t cap = std::max<size_t>(need + need / 2, 1 << 16);
+    size_t cap = std::max<size_t>(need + need / 2, min_bytes);
     void* np = nullptr;
     TFIM_TRY(dev_alloc(&np, cap, s));
     if (b.p && b.bytes) TFIM_CUDA(cudaMemcpyAsync(np, b.p, b.bytes, cudaMemcpyDeviceToDevice, s));
@@ -877,22 +1016,87 @@ int grow(Pool& b, size_t need, cudaStream_t s) {
     return TFIM_OK;
 }
 
+// The captured wave loop.  Its launches read ResArgs at `args` and sizes from the status
+// record at `status`; it is rebuilt when either moves or the set of counters changes.
+struct WaveGraph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    const void* args = nullptr;
+    const void* status = nullptr;
+    int with_proj = -1;
+    void release() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+        args = status = nullptr;
+        with_proj = -1;
+    }
+};
+
+int build_wave_graph(WaveGraph& G, const ResArgs* d_args, ResStatus* d_status, bool with_proj, const int64_t* red_off,
+                     const int32_t* red_items, cudaStream_t s) {
+    G.release();
+    int sm = 148, dev = 0, occ3 = 1, occ1 = 1, occp = 1, occe = 1;
+    TFIM_CUDA(cudaGetDevice(&dev));
+    TFIM_CUDA(cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, dev));
+    TFIM_TRY(persistent_occupancy(&occ3, &occ1, &occp));
+    TFIM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occe, k_res_expand_g, 256, 0));
+    TFIM_CUDA(cudaGraphCreate(&G.graph, 0));
+    cudaGraphConditionalHandle h;
+    TFIM_CUDA(cudaGraphConditionalHandleCreate(&h, G.graph, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    TFIM_CUDA(cudaGraphAddNode(&node, G.graph, nullptr, 0, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    TFIM_CUDA(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    int rc = TFIM_OK;
+    do {
+        k_res_pack_g<<<1, kPackThreads, 0, s>>>(d_args);
+        k_res_zero<<<sm * 4, 256, 0, s>>>(d_args);
+        if ((rc = launch_count_lop3_persistent(&d_args->a3, &d_status->tiles_l3, sm * std::max(1, occ3), s))) break;
+        if ((rc = launch_count_b1_persistent(&d_args->a1, &d_status->tiles_b1, sm * std::max(1, occ1), s))) break;
+        if (with_proj &&
+            (rc = launch_count_proj_persistent(&d_args->a3, &d_status->n_proj, sm * std::max(1, occp), red_off, red_items, s)))
+            break;
+        k_res_expand_g<<<sm * std::max(1, occe), 256, 0, s>>>(d_args);
+        k_res_control<<<1, 32, 0, s>>>(d_args, h);
+    } while (0);
+    cudaGraph_t captured = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(s, &captured);
+    if (rc != TFIM_OK) return rc;
+    TFIM_CUDA(ec);
+    TFIM_CUDA(cudaGetLastError());
+    TFIM_CUDA(cudaGraphInstantiate(&G.exec, G.graph, 0));
+    G.args = d_args;
+    G.status = d_status;
+    G.with_proj = with_proj ? 1 : 0;
+    return TFIM_OK;
+}
+
 }  // namespace
 
 struct ResidentState {
     Pool fams, items, heads, stack, looks, free_slots, defer, mfi_off, mfi_len, mfi_sup, mfi_items, log_feat, log_label;
     Pool djobs, jobs, rows, row_job, row_local, tiles_l3, tiles_b1, counts, status, is_root, dense_freq, top_pos, top_diag,
-        proj_list;
-    HostBuf h_status;
+        proj_list, args;
+    HostBuf h_status, h_args;
+    WaveGraph graph;
+    int32_t launch_id = 0;
     void release(cudaStream_t s) {
+        graph.release();
         for (Pool* b : {&fams, &items, &heads, &stack, &looks, &free_slots, &defer, &mfi_off, &mfi_len, &mfi_sup, &mfi_items,
                         &log_feat, &log_label, &djobs, &jobs, &rows, &row_job, &row_local, &tiles_l3, &tiles_b1, &counts,
-                        &status, &is_root, &dense_freq, &top_pos, &top_diag, &proj_list}) {
+                        &status, &is_root, &dense_freq, &top_pos, &top_diag, &proj_list, &args}) {
             dev_free(b->p, s);
             b->p = nullptr;
             b->bytes = 0;
         }
         h_status.release();
+        h_args.release();
     }
 };
 
@@ -935,14 +1139,18 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
     }
     const int32_t wave_rows = o->wave_cap > 0 ? o->wave_cap : 4096;
     const int64_t top_out = (int64_t)n0 * n0;
-    int64_t cap_out = std::max<int64_t>(top_out, 64LL << 20);
-    int64_t cap_tiles = 1LL << 21;
+    const bool small = o->small_pools != 0;
+    const size_t gmin = small ? 64 : (1 << 16);
+    auto grow = [&](Pool& b, size_t need, cudaStream_t st) { return tfim::grow(b, need, st, gmin); };
+    int64_t cap_out = small ? top_out : std::max<int64_t>(top_out, 64LL << 20);
+    int64_t cap_tiles = small ? 64 : 1LL << 21;
     int64_t cap_rows = std::max<int64_t>(wave_rows, n0) + 64;
 
-    // initial capacities
-    int64_t cap_fam = std::max<int64_t>(4 * n0, 1 << 16);
-    int64_t cap_item = std::max<int64_t>(4 * top_out + 2 * n0, 1 << 20);
+    // initial capacities (the first wave's ensure grows them to what its expand needs)
+    int64_t cap_fam = small ? 1 : std::max<int64_t>(4 * n0, 1 << 16);
+    int64_t cap_item = small ? n0 : std::max<int64_t>(4 * top_out + 2 * n0, 1 << 20);   // holds the top family's list
     int64_t cap_head = 1 << 20, cap_mfi = 1 << 16, cap_mfi_items = 1 << 20, cap_slots = 1 << 12, cap_log = 1 << 16;
+    if (small) cap_head = cap_mfi = cap_mfi_items = cap_slots = cap_log = 1;
     TFIM_TRY(grow(R.status, sizeof(ResStatus), s));
     TFIM_TRY(grow(R.fams, cap_fam * sizeof(DFam), s));
     TFIM_TRY(grow(R.items, cap_item * 4, s));
@@ -1060,16 +1268,31 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
             P.mlp_w = (const __nv_bfloat16*)wb;
             P.mlp_p = pp;
         }
+        Caps& k = P.caps;
+        k.fam = (int64_t)std::min(R.fams.bytes / sizeof(DFam), R.stack.bytes / 4);
+        k.item = (int64_t)(R.items.bytes / 4);
+        k.head = (int64_t)(R.heads.bytes / 4);
+        k.mfi = (int64_t)std::min({R.mfi_off.bytes, R.mfi_len.bytes, R.mfi_sup.bytes}) / 4;
+        k.mfi_items = (int64_t)(R.mfi_items.bytes / 4);
+        k.looks = (int64_t)(R.looks.bytes / sizeof(DLook));
+        k.slots = std::min<int64_t>(slot_cap, (int64_t)std::min(R.free_slots.bytes, R.defer.bytes) / 4);
+        k.log = o->log_lookahead ? (int64_t)std::min(R.log_feat.bytes / 128, R.log_label.bytes / 4) : 0;
+        k.rows = cap_rows;
+        P.row_bytes = row_bytes;
+        P.wave_limit = 0x7fffffff;
+        P.launch_id = 0;
+        P.max_launch_ns = 2000000000ull;
     };
     // capacity for the worst case of one expand over `rows` rows of at most `max_cols`
     // columns each and `out_total` counts
-    auto ensure = [&](const ResStatus& h) -> int {
-        const int64_t rows = h.rows;
+    auto ensure = [&](const ResStatus& h, int64_t rows, int64_t jobs, int64_t out_total, int64_t max_head,
+                      int64_t max_cols) -> int {
+        const int64_t list = max_head + 2 + max_cols;
         const int64_t need_fam = h.fam_n + rows + 1;
-        const int64_t need_item = h.item_n + 2 * h.out_total + rows + 1;
-        const int64_t need_head = h.head_n + rows * (int64_t)(h.max_head + 2 + h.max_cols) + 1;
-        const int64_t need_mfi = h.mfi_n + rows + h.jobs + 1;
-        const int64_t need_mfi_items = h.mfi_item_n + (rows + h.jobs) * (int64_t)(h.max_head + 2 + h.max_cols) + 1;
+        const int64_t need_item = h.item_n + 2 * out_total + rows + 1;
+        const int64_t need_head = h.head_n + rows * list + 1;
+        const int64_t need_mfi = h.mfi_n + rows + jobs + 1;
+        const int64_t need_mfi_items = h.mfi_item_n + (rows + jobs) * list + 1;
         const int64_t need_slots = h.slot_n + 2 * rows + 2;
         const int64_t need_log = h.log_n + rows + 1;
         TFIM_TRY(grow(R.fams, need_fam * sizeof(DFam), s));
@@ -1101,10 +1324,32 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
         refresh_ptrs();
         return TFIM_OK;
     };
+    // the pack declined a wave: grow what it asked for
+    auto grow_for = [&](const ResStatus& h) -> int {
+        if (h.starved) {
+            // a single row does not fit the count buffer
+            cap_out *= 4;
+            TFIM_TRY(grow(R.counts, cap_out * 4, s));
+        }
+        if (h.grow) {
+            if (h.g_out > cap_out) {
+                cap_out = std::max<int64_t>(2 * cap_out, h.g_out);
+                TFIM_TRY(grow(R.counts, cap_out * 4, s));
+            }
+            if (h.g_tiles > cap_tiles) {
+                cap_tiles = std::max<int64_t>(2 * cap_tiles, h.g_tiles);
+                TFIM_TRY(grow(R.tiles_l3, cap_tiles * sizeof(TileDesc), s));
+                TFIM_TRY(grow(R.tiles_b1, cap_tiles * sizeof(TileDesc), s));
+            }
+            TFIM_TRY(ensure(h, h.g_rows, h.g_jobs, h.g_out, h.g_max_head, h.g_max_cols));
+        }
+        refresh_ptrs();   // the next pack clears the request
+        return TFIM_OK;
+    };
 
     // wave 1: the top family, counted whole
     *hst = hs;
-    TFIM_TRY(ensure(hs));
+    TFIM_TRY(ensure(hs, hs.rows, hs.jobs, hs.out_total, 0, hs.max_cols));
     {
         std::vector<TileDesc> tl;
         if (top_mode == 1) {
@@ -1158,7 +1403,50 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
         kernel_ms += ms;
     }
     // following waves
-    while (true) {
+    const bool use_graph = o->use_graphs != 0;
+    int64_t host_waves = 0;
+    if (use_graph) {
+        TFIM_TRY(grow(R.args, sizeof(ResArgs), s));
+        TFIM_TRY(R.h_args.reserve(sizeof(ResArgs)));
+        const bool with_proj = c->csr_exact && (o->counter == TFIM_COUNTER_PROJ || (o->counter == TFIM_COUNTER_AUTO && P.proj_auto));
+        ResArgs* d_args = (ResArgs*)R.args.p;
+        if (!R.graph.exec || R.graph.args != R.args.p || R.graph.status != R.status.p || R.graph.with_proj != (int)with_proj)
+            TFIM_TRY(build_wave_graph(R.graph, d_args, (ResStatus*)R.status.p, with_proj, c->d_red_off, c->d_red_items, s));
+        int64_t slices = 0;
+        while (true) {
+            ResArgs* ha = R.h_args.as<ResArgs>();
+            ha->p = P;
+            ha->p.launch_id = ++R.launch_id;
+            ha->p.wave_limit = 0x7fffffff;
+            CountArgs a;
+            a.bitmap = c->d_bitmap; a.W = W; a.masks = P.masks; a.jobs = P.jobs; a.rows = P.rows;
+            a.cols = P.items; a.out = P.counts; a.n_tiles = 0; a.job_list = P.proj_list;
+            a.tiles = P.tiles_l3;
+            ha->a3 = a;
+            a.tiles = P.tiles_b1;
+            ha->a1 = a;
+            TFIM_CUDA(cudaMemcpyAsync(d_args, ha, sizeof(ResArgs), cudaMemcpyHostToDevice, s));
+            TFIM_CUDA(cudaGraphLaunch(R.graph.exec, s));
+            launches++;
+            slices++;
+            TFIM_CUDA(cudaMemcpyAsync(hst, R.status.p, sizeof(ResStatus), cudaMemcpyDeviceToHost, s));
+            const double ts = std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+            TFIM_CUDA(cudaStreamSynchronize(s));
+            sync_ms += (std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count() - ts) * 1e3;
+            TFIM_CHECK(hst->error == 0, TFIM_E_STATE, "resident search invariant failed (code %d)", hst->error);
+            if (hst->starved || hst->grow) {
+                TFIM_TRY(grow_for(*hst));
+                continue;
+            }
+            if (hst->jobs == 0) break;   // the stack and the lookahead queue are empty
+            TFIM_CHECK(slices < (1LL << 40), TFIM_E_STATE, "resident search did not finish");
+        }
+        // per wave: pack, zero, lop3, b1, [proj], expand, control
+        launches += (int64_t)hst->waves * (6 + (with_proj ? 1 : 0));
+        count_launches += (int64_t)hst->waves * (2 + (with_proj ? 1 : 0));
+        kernel_ms += (double)hst->count_ns * 1e-6;
+    }
+    while (!use_graph) {
         k_res_pack<<<1, kPackThreads, 0, s>>>(P);
         TFIM_CUDA(cudaGetLastError());
         launches++;
@@ -1167,21 +1455,15 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
         TFIM_CUDA(cudaStreamSynchronize(s));
         sync_ms += (std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count() - ts) * 1e3;
         TFIM_CHECK(hst->error == 0, TFIM_E_STATE, "resident search invariant failed (code %d)", hst->error);
-        if (hst->starved) {
-            // a single row does not fit the count buffer: enlarge it and retry the pack
-            cap_out *= 4;
-            TFIM_TRY(grow(R.counts, cap_out * 4, s));
-            hst->starved = 0;
-            TFIM_CUDA(cudaMemcpyAsync(R.status.p, hst, sizeof(ResStatus), cudaMemcpyHostToDevice, s));
-            refresh_ptrs();
+        if (hst->starved || hst->grow) {
+            TFIM_TRY(grow_for(*hst));
             continue;
         }
         if (hst->jobs == 0) break;
-        TFIM_TRY(ensure(*hst));
         TFIM_CUDA(cudaMemsetAsync(R.counts.p, 0, (size_t)hst->out_total * 4, s));
         CountArgs a;
         a.bitmap = c->d_bitmap; a.W = W; a.masks = c->d_masks.as<uint32_t>(); a.jobs = P.jobs; a.rows = P.rows;
-        a.cols = P.items; a.out = P.counts;
+        a.cols = P.items; a.out = P.counts; a.job_list = P.proj_list;
         TFIM_CUDA(cudaEventRecord(c->ev0, s));
         if (hst->tiles_l3) {
             a.tiles = P.tiles_l3;
@@ -1203,17 +1485,17 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
             count_launches++;
         }
         TFIM_CUDA(cudaEventRecord(c->ev1, s));
-        bytes_alg += row_bytes * (2LL * hst->rows + hst->jobs) + 4 * hst->out_total;   // rows, columns ~ rows, bases
         const int64_t threads = (int64_t)hst->rows * 32;
         k_res_expand<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(P);
         TFIM_CUDA(cudaGetLastError());
         launches++;
-        waves++;
+        host_waves++;
         float ms = 0;
         TFIM_CUDA(cudaEventSynchronize(c->ev1));
         cudaEventElapsedTime(&ms, c->ev0, c->ev1);
         kernel_ms += ms;
     }
+    waves += use_graph ? (int64_t)hst->waves : host_waves;
     // results
     const ResStatus fin = *hst;
     std::vector<int32_t> moff(fin.mfi_n), mlen(fin.mfi_n), msup(fin.mfi_n), mitems(fin.mfi_item_n);
@@ -1247,7 +1529,7 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
     stt->count_launches += count_launches;
     stt->kernel_ms += kernel_ms;
     stt->sync_ms += sync_ms;
-    stt->bytes_alg += bytes_alg;
+    stt->bytes_alg += bytes_alg + (int64_t)fin.bytes_alg;
     stt->bit_ops = stt->supports * c->n_bits;
     (void)t_host0;
     return TFIM_OK;

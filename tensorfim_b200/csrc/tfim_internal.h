@@ -122,7 +122,7 @@ constexpr double kTuneHbmBytes = 6.5e12;       // bytes/s
 constexpr int kTuneProjAuto = 0;               // projected counter in the automatic choice
 
 constexpr int kLop3Rows = 8;        // rows per CUDA-core tile
-constexpr int kLop3Chunk = 1024;    // max words per CUDA-core tile
+constexpr int kLop3Chunk = 4096;    // word slice of a CUDA-core tile in tfim_count_wave
 constexpr int kB1Rows = 64;         // rows per tensor-core tile
 constexpr int kB1Cols = 64;         // columns per tensor-core tile
 
@@ -136,10 +136,21 @@ struct CountArgs {
     const TileDesc* tiles;
     int32_t n_tiles;
     int32_t* out;
+    const int32_t* job_list;   // projected counter: the jobs it counts
 };
 
 int launch_count_lop3(const CountArgs& a, cudaStream_t s);
 int launch_count_b1(const CountArgs& a, cudaStream_t s);
+// Persistent forms for waves built on the GPU: the arguments and the tile / job count are
+// read from device memory and a fixed grid strides over the tiles, so the launches do not
+// depend on the wave and can be captured once in a graph.
+int launch_count_lop3_persistent(const CountArgs* d_args, const int32_t* d_n_tiles, int32_t grid, cudaStream_t s);
+int launch_count_b1_persistent(const CountArgs* d_args, const int32_t* d_n_tiles, int32_t grid, cudaStream_t s);
+int launch_count_proj_persistent(const CountArgs* d_args, const int32_t* d_n_jobs, int32_t grid, const int64_t* red_off,
+                                 const int32_t* red_items, cudaStream_t s);
+// blocks of each persistent kernel resident per SM
+int persistent_occupancy(int* lop3, int* b1, int* proj);
+int configure_count_kernels();
 int launch_pair_count(const int64_t* red_off, const int32_t* red_items, int64_t n_red, const int32_t* pos,
                       int32_t nF, int32_t* M, cudaStream_t s);
 int launch_mirror(int32_t* M, int32_t nF, const int32_t* diag, cudaStream_t s);

@@ -157,9 +157,13 @@ class Database:
         return x, y
 
     def mine(self, engine: str = "batched", counter: str = "auto", lookahead=True,
-             wave_cap: int = 0, top: str = "auto", log_lookahead: bool = False, proj_auto: int = -1) -> MineResult:
+             wave_cap: int = 0, top: str = "auto", log_lookahead: bool = False, proj_auto: int = -1,
+             graphs: bool = False, small_pools: bool = False) -> MineResult:
         """lookahead: False/"off", True/"filtered" (every node passing the exact tail-pair
-        filter), "learned" (the attached proposal, or the shipped weights), "all"."""
+        filter), "learned" (the attached proposal, or the shipped weights), "all".
+        graphs: (resident engine) run the wave loop as a captured CUDA graph whose conditional
+        WHILE node repeats pack -> count -> expand on the device; the host reads the status
+        only when the search ends or a pool has to grow."""
         o = _lib.MineOpts()
         lib().tfim_mine_opts_default(C.byref(o))
         o.engine = ENGINES[engine]
@@ -173,6 +177,8 @@ class Database:
         o.proj_auto = int(proj_auto)
         o.wave_cap = int(wave_cap)
         o.top_counter = {"auto": 0, "bitmap": 1, "pairs": 2}[top]
+        o.use_graphs = int(bool(graphs))
+        o.small_pools = int(bool(small_pools))
         st = _lib.MineStats()
         check(lib().tfim_mine(self._h, C.byref(o), C.byref(st)))
         n = lib().tfim_num_mfis(self._h)

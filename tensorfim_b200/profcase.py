@@ -2,6 +2,7 @@
 
     python -m tensorfim_b200.profcase --cfg 4 --scale 0.25 --counter tensor [--engine batched|resident|plain]
                                       [--top auto|bitmap|pairs] [--lookahead off|filtered|learned|all]
+                                      [--graphs] [--repeat N]
 
 Generates the configuration's database (tensorfim_b200.synth) at the given row scale,
 builds it on cuda:0 and mines it once; prints the MFI count and the engine statistics.
@@ -25,13 +26,14 @@ def main() -> None:
     ap.add_argument("--top", default="auto")
     ap.add_argument("--lookahead", default="learned", choices=["off", "filtered", "learned", "all"])
     ap.add_argument("--repeat", type=int, default=1)
+    ap.add_argument("--graphs", action="store_true", help="resident engine: wave loop as a CUDA graph")
     a = ap.parse_args()
     kw = {"scale": a.scale} if a.cfg != 3 else {"scale": a.scale, "replicas": 1}
     db0 = synth.generate(a.cfg, **kw)
     minsup = a.minsup if a.minsup is not None else MINSUP[a.cfg]
     with Database.from_csr(db0.offsets, db0.items, minsup) as db:
         for _ in range(a.repeat):
-            r = db.mine(engine=a.engine, counter=a.counter, top=a.top, lookahead=a.lookahead)
+            r = db.mine(engine=a.engine, counter=a.counter, top=a.top, lookahead=a.lookahead, graphs=a.graphs)
         print(json.dumps({"mfis": len(r.mfis), "info": db.info, "stats": r.stats}))
 
 

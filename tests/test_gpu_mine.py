@@ -30,6 +30,10 @@ VARIANTS = [
     dict(engine="resident", counter="auto", lookahead=True, top="pairs"),
     dict(engine="resident", counter="proj", lookahead="learned"),
     dict(engine="resident", counter="proj", lookahead="all", wave_cap=29),
+    dict(engine="resident", counter="auto", lookahead=True, graphs=True),
+    dict(engine="resident", counter="tensor", lookahead="all", wave_cap=37, graphs=True),
+    dict(engine="resident", counter="lop3", lookahead="learned", top="bitmap", graphs=True),
+    dict(engine="resident", counter="proj", lookahead="all", wave_cap=29, graphs=True),
 ]
 PLAIN_OK = {"cfg1_full", "cfg2_full", "cfg3_base", "cfg3_base_t30", "cfg4_s001", "cfg5_s002", "edge_dups",
             "edge_format", "edge_identical", "edge_item0", "edge_none", "edge_single", "edge_ties"}
@@ -104,6 +108,7 @@ def test_cfg4_scaled_matches_oracle(oracle_mod, tmp_path):
     with tf.Database.from_csr(db0.offsets, db0.items, 0.002) as db:
         for counter in ("auto", "lop3", "tensor"):
             assert db.mine(counter=counter).as_dict() == exp
+        assert db.mine(engine="resident", graphs=True).as_dict() == exp
 
 
 @pytest.mark.slow
@@ -115,6 +120,22 @@ def test_cfg4_full_size_certified():
         _certify(db, res.mfis, db.dense_to_orig())
         assert db.mine(engine="resident").as_dict() == res.as_dict()
         assert db.mine(engine="resident", lookahead="learned").as_dict() == res.as_dict()
+        g = db.mine(engine="resident", lookahead="learned", graphs=True)
+        assert g.as_dict() == res.as_dict()
+        assert g.stats["waves"] > 1
+
+
+@pytest.mark.parametrize("graphs", [False, True])
+@pytest.mark.parametrize("name", ["cfg1_full", "cfg4_s001", "cfg5_s002", "edge_ties"])
+def test_resident_pool_growth(tmp_path, name, graphs):
+    """Start every pool of the resident engine at its minimum, so that the pack declines
+    waves that do not fit and the host grows the pools mid-search; results unchanged."""
+    fx = load_golden(name)
+    path = golden_input(fx, tmp_path)
+    with tf.Database.from_file(path, fx["spec"]["minsup"]) as db:
+        for la in ("filtered", "all"):
+            res = db.mine(engine="resident", lookahead=la, graphs=graphs, small_pools=True, log_lookahead=True)
+            assert res.as_dict() == fx["expected"], (la, graphs)
 
 
 @pytest.mark.slow
