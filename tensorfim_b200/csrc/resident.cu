@@ -46,7 +46,8 @@ struct DLook {
 enum { kJobFam = 0, kJobLook = 1 };
 struct DJob {
     int32_t fam, kind, r0, nr, slot, log;
-    int32_t b3, b1;            // exclusive prefix of base CUDA-core / tensor-core tiles over the wave's jobs
+    int32_t b3, b1;            // exclusive prefix of CUDA-core / tensor-core tiles over the wave's jobs
+    int32_t cls, sl3;          // counter (0 CUDA-core, 1 tensor-core, 2 projected); word slices of its CUDA-core tiles
 };
 
 struct ResStatus {
@@ -253,6 +254,7 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
             const DFam f = p.fams[L.fam];
             DJob dj;
             dj.fam = L.fam; dj.kind = kJobLook; dj.r0 = 0; dj.nr = 1; dj.slot = L.slot; dj.log = L.log; dj.b3 = 0; dj.b1 = 0;
+            dj.cls = 0; dj.sl3 = 1;
             p.djobs[k] = dj;
             JobDesc jd;
             jd.base_slot = -1; jd.base_item = -1; jd.n_rows = 1; jd.n_cols = f.nF - f.nT + 1;
@@ -356,6 +358,7 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
             const int32_t jid = s_n_jobs + (int32_t)hx[q];
             DJob dj;
             dj.fam = fid; dj.kind = kJobFam; dj.r0 = f.next_row; dj.nr = take[q]; dj.slot = -1; dj.log = -1; dj.b3 = 0; dj.b1 = 0;
+            dj.cls = 0; dj.sl3 = 1;
             p.djobs[jid] = dj;
             JobDesc jd;
             jd.base_slot = f.slot; jd.base_item = f.item; jd.n_rows = take[q]; jd.n_cols = f.nF;
@@ -396,55 +399,100 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
         p.row_job[g] = j;
         p.row_local[g] = r;
     }
-    // (4) tiles: base tiles per job, prefix over jobs (chunks of kPackCand)
-    int64_t tot3 = 0, tot1 = 0;
+    // (4) tiles.  Pass 1 picks each job's counter and sums the estimated cost of its
+    // CUDA-core tiles; pass 2 gives every CUDA-core job its own number of word slices (a
+    // heavy job -- dense prefix, many rows and columns -- is split so that no tile runs
+    // far longer than the wave's average) and forms the prefix sums the tile writers
+    // search.  Tensor-core jobs share one split-k factor.
+    const int64_t W = p.W;
+    const float P4 = (float)(W >> 2);
+    auto l3_cost = [&](const JobDesc& jd, const DJob& dj) -> float {
+        float d = 1.f;   // fraction of 128-bit base positions that are nonzero
+        if (dj.kind == kJobFam && (jd.base_slot >= 0 || jd.base_item >= 0) && p.n_bits > 0)
+            d = fminf(1.f, 128.f * (float)p.fams[dj.fam].sup / (float)p.n_bits);
+        const float nr = (float)min(jd.n_rows, kLop3Rows), nc = (float)min(jd.n_cols, 64);
+        return P4 * (1.f + d * (2.f + nr + nr * nc / 32.f));
+    };
+    float cost_local = 0.f;
+    int64_t tot1 = 0;
     for (int base = 0; base < nj; base += kPackCand) {
-        int64_t a3[kPackItems], a1[kPackItems], x3[kPackItems], x1[kPackItems];
+        int64_t a1[kPackItems], x1[kPackItems];
         for (int q = 0; q < kPackItems; q++) {
             const int j = base + tid * kPackItems + q;
-            a3[q] = a1[q] = 0;
+            a1[q] = 0;
             if (j < nj) {
                 const JobDesc jd = p.jobs[j];
-                const DJob djq = p.djobs[j];
-                const bool fam = djq.kind == kJobFam;
-                if (fam && use_proj(p, jd, p.fams[djq.fam].sup)) {
+                DJob* djp = p.djobs + j;
+                const bool fam = djp->kind == kJobFam;
+                int cls = 0;
+                if (fam && use_proj(p, jd, p.fams[djp->fam].sup)) {
+                    cls = 2;
                     const int32_t k = atomicAdd(&p.st->n_proj, 1);
                     p.proj_list[k] = j;
                 } else if (use_b1_shape(p, jd.n_rows, jd.n_cols) && fam) {
+                    cls = 1;
                     a1[q] = b1_tiles(jd.n_rows, jd.n_cols);
                 } else {
-                    a3[q] = l3_tiles(jd.n_rows, jd.n_cols);
+                    cost_local += (float)l3_tiles(jd.n_rows, jd.n_cols) * l3_cost(jd, *djp);
+                }
+                djp->cls = cls;
+            }
+        }
+        Scan(tmp.scan).ExclusiveSum(a1, x1, s_agg);
+        __syncthreads();
+        const int64_t g1 = s_agg;
+        for (int q = 0; q < kPackItems; q++) {
+            const int j = base + tid * kPackItems + q;
+            if (j < nj) p.djobs[j].b1 = (int32_t)(tot1 + x1[q]);
+        }
+        tot1 += g1;
+        __syncthreads();
+    }
+    __shared__ float s_cost;
+    {
+        typedef cub::BlockReduce<float, kPackThreads> RedF;
+        __shared__ typename RedF::TempStorage redf;
+        const float c = RedF(redf).Sum(cost_local);
+        if (tid == 0) s_cost = c;
+        __syncthreads();
+    }
+    // about 8 tile slices per SM: two rounds of the 4 resident blocks
+    const float target = fmaxf(s_cost / (8.f * (float)p.sm_count), 1.f);
+    const int64_t max_sl = lmax(1, W / 256);
+    int64_t tot3 = 0;
+    for (int base = 0; base < nj; base += kPackCand) {
+        int64_t a3[kPackItems], x3[kPackItems];
+        for (int q = 0; q < kPackItems; q++) {
+            const int j = base + tid * kPackItems + q;
+            a3[q] = 0;
+            if (j < nj) {
+                const JobDesc jd = p.jobs[j];
+                DJob* djp = p.djobs + j;
+                if (djp->cls == 0) {
+                    int64_t sl = lmin(max_sl, lmax(1, (int64_t)ceilf(l3_cost(jd, *djp) / target)));
+                    const int64_t wsl = ((W / 64 + sl - 1) / sl) * 64;
+                    sl = wsl > 0 ? (W + wsl - 1) / wsl : 1;
+                    djp->sl3 = (int32_t)sl;
+                    a3[q] = l3_tiles(jd.n_rows, jd.n_cols) * sl;
                 }
             }
         }
         Scan(tmp.scan).ExclusiveSum(a3, x3, s_agg);
         __syncthreads();
         const int64_t g3 = s_agg;
-        Scan(tmp.scan).ExclusiveSum(a1, x1, s_agg);
-        __syncthreads();
-        const int64_t g1 = s_agg;
         for (int q = 0; q < kPackItems; q++) {
             const int j = base + tid * kPackItems + q;
-            if (j >= nj) continue;
-            // b3/b1 hold the prefix; a job's own count is recomputed from its shape
-            p.djobs[j].b3 = (int32_t)(tot3 + x3[q]);
-            p.djobs[j].b1 = (int32_t)(tot1 + x1[q]);
+            if (j < nj) p.djobs[j].b3 = (int32_t)(tot3 + x3[q]);
         }
         tot3 += g3;
-        tot1 += g1;
         __syncthreads();
     }
-    const int64_t W = p.W;
     int64_t ks1 = tot1 > 0 ? lmax(1, (4LL * p.sm_count + tot1 - 1) / tot1) : 1;
     ks1 = lmin(ks1, lmax(1, W / 64));
     int64_t kslice = ((W / 64 + ks1 - 1) / ks1) * 64;
-    int64_t ws3 = tot3 > 0 ? lmax(1, (8LL * p.sm_count + tot3 - 1) / tot3) : 1;
-    ws3 = lmin(ws3, lmax(1, W / 256));
-    int64_t wslice = ((W / 64 + ws3 - 1) / ws3) * 64;
     if (kslice <= 0) kslice = 64;
-    if (wslice <= 0) wslice = 64;
-    const int64_t nk = W > 0 ? (W + kslice - 1) / kslice : 1, nw = W > 0 ? (W + wslice - 1) / wslice : 1;
-    const int64_t T3 = tot3 * nw, T1 = tot1 * nk;
+    const int64_t nk = W > 0 ? (W + kslice - 1) / kslice : 1;
+    const int64_t T3 = tot3, T1 = tot1 * nk;
     // the wave is committed only when the worst case of its expand fits the pools
     if (tid == 0) {
         const bool fit = s_out_total <= p.cap_out && T1 <= p.cap_tiles && T3 <= p.cap_tiles &&
@@ -474,15 +522,18 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
     }
     if (T3 <= p.cap_tiles)
         for (int64_t t = tid; t < T3; t += kPackThreads) {
-            const int64_t slice = t / tot3, local = t % tot3;
-            const int j = find_job_by_tile<false>(p.djobs, nj, local);
+            const int j = find_job_by_tile<false>(p.djobs, nj, t);
             const JobDesc jd = p.jobs[j];
-            const int64_t within = local - p.djobs[j].b3;
+            const DJob dj = p.djobs[j];
+            const int64_t local = t - dj.b3;
+            const int64_t bt = l3_tiles(jd.n_rows, jd.n_cols);
+            const int64_t slice = local / bt, within = local % bt;
+            const int64_t wsl = ((W / 64 + dj.sl3 - 1) / dj.sl3) * 64;
             const int cg = (jd.n_cols + 63) / 64;
             const int rg = (int)(within / cg), cc = (int)(within % cg);
-            const int64_t w0 = slice * wslice;
+            const int64_t w0 = slice * wsl;
             p.tiles_l3[t] = TileDesc{j, rg * kLop3Rows, min(kLop3Rows, jd.n_rows - rg * kLop3Rows), cc * 64,
-                                     min(jd.n_cols, cc * 64 + 64), (int32_t)w0, (int32_t)lmin(W, w0 + wslice), 0};
+                                     min(jd.n_cols, cc * 64 + 64), (int32_t)w0, (int32_t)lmin(W, w0 + wsl), 0};
         }
     if (T1 <= p.cap_tiles)
         for (int64_t t = tid; t < T1; t += kPackThreads) {
@@ -1203,7 +1254,7 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
     hs.supports = (unsigned long long)top_out;
     {
         std::vector<DJob> dj(1);
-        dj[0] = DJob{0, kJobFam, 0, n0, -1, -1, 0, 0};
+        dj[0] = DJob{0, kJobFam, 0, n0, -1, -1, 0, 0, 0, 1};
         std::vector<JobDesc> jd(1);
         jd[0] = JobDesc{-1, -1, n0, n0, 0, 0, 0, -1, 0};
         std::vector<RowDesc> rows(n0);
