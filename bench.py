@@ -265,7 +265,7 @@ def main() -> int:
             t1 = time.perf_counter()
             if k >= max(1, args.warmup):
                 e2e_ms.append((t1 - t0) * 1000.0)
-            d2h = sum(4 * len(items) + 12 for items, _ in res.mfis) + 8
+            d2h = res.items.nbytes + res.offsets.nbytes + res.supports.nbytes
         e2e_t = max_over_ranks(statistics.mean(e2e_ms))
         e2e = {"value": world * ref_supports / (e2e_t / 1000.0), "unit": "supports/s", "h2d_bytes_per_step": int(h2d_bytes),
                "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_t,
@@ -315,7 +315,7 @@ def main() -> int:
         "plain_mine_time_s": plain.stats["device_ms"] / 1000.0 if plain else None,
         "speedup_vs_plain": (plain.stats["device_ms"] / ms) if plain else None,
         "set_identical_to_plain": identical,
-        "n_mfi": len(batched.mfis),
+        "n_mfi": len(batched),
         "reference_supports_per_db": ref_supports,
         "counted_supports_per_db": batched.stats["supports"],
         "stats": {k: v for k, v in batched.stats.items()},

@@ -264,8 +264,7 @@ int tfim_mine(tfim_ctx* c, const tfim_mine_opts* opts, tfim_mine_stats* stats) {
     else tfim_mine_opts_default(&o);
     tfim_mine_stats st;
     memset(&st, 0, sizeof st);
-    c->mfi_items.clear();
-    c->mfi_support.clear();
+    c->mfis.clear();
     c->mined = false;
     cudaEvent_t e_begin = nullptr, e_end = nullptr;
     TFIM_CUDA(cudaEventCreate(&e_begin));
@@ -287,21 +286,26 @@ int tfim_mine(tfim_ctx* c, const tfim_mine_opts* opts, tfim_mine_stats* stats) {
     if (rc != TFIM_OK) return rc;
     st.device_ms = span_ms;
     st.host_ms = std::chrono::duration<double, std::milli>(t1 - t0).count() - st.sync_ms;
-    // descending support; ties by descending item lists (deterministic order)
-    std::vector<size_t> idx(c->mfi_items.size());
-    std::iota(idx.begin(), idx.end(), 0);
-    std::sort(idx.begin(), idx.end(), [&](size_t a, size_t b) {
-        if (c->mfi_support[a] != c->mfi_support[b]) return c->mfi_support[a] > c->mfi_support[b];
-        return c->mfi_items[a] > c->mfi_items[b];
-    });
-    std::vector<std::vector<int32_t>> items(idx.size());
-    std::vector<int32_t> sup(idx.size());
-    for (size_t k = 0; k < idx.size(); k++) { items[k] = std::move(c->mfi_items[idx[k]]); sup[k] = c->mfi_support[idx[k]]; }
-    c->mfi_items.swap(items);
-    c->mfi_support.swap(sup);
-    st.mine_seconds = std::chrono::duration<double>(t1 - t0).count();
-    if (st.bit_ops == 0) st.bit_ops = st.supports * c->n_bits;
-    st.n_mfi = (int64_t)c->mfi_items.size();
+    {
+        // descending support; ties by descending item lists (deterministic order)
+        const MfiSet& M = c->mfis;
+        std::vector<int32_t> idx(M.size());
+        std::iota(idx.begin(), idx.end(), 0);
+        std::sort(idx.begin(), idx.end(), [&](int32_t a, int32_t b) {
+            if (M.sup[a] != M.sup[b]) return M.sup[a] > M.sup[b];
+            return std::lexicographical_compare(M.items.begin() + M.off[b], M.items.begin() + M.off[b + 1],
+                                                M.items.begin() + M.off[a], M.items.begin() + M.off[a + 1]);
+        });
+        MfiSet S;
+        S.items.reserve(M.items.size());
+        S.off.reserve(M.size() + 1);
+        S.sup.reserve(M.size());
+        for (int32_t k : idx) S.add(M.items.data() + M.off[k], (size_t)(M.off[k + 1] - M.off[k]), M.sup[k]);
+        c->mfis.items.swap(S.items);
+        c->mfis.off.swap(S.off);
+        c->mfis.sup.swap(S.sup);
+    }
+    st.n_mfi = (int64_t)c->mfis.size();
     c->mined = true;
     c->last_stats = st;
     if (stats) *stats = st;
@@ -327,25 +331,18 @@ int64_t tfim_lookahead_log(const tfim_ctx* c, float* feats, float* labels, int64
     return n;
 }
 
-int64_t tfim_num_mfis(const tfim_ctx* c) { return c && c->mined ? (int64_t)c->mfi_items.size() : -1; }
+int64_t tfim_num_mfis(const tfim_ctx* c) { return c && c->mined ? (int64_t)c->mfis.size() : -1; }
 
-int64_t tfim_mfi_item_total(const tfim_ctx* c) {
-    if (!c || !c->mined) return -1;
-    int64_t s = 0;
-    for (auto& v : c->mfi_items) s += (int64_t)v.size();
-    return s;
-}
+int64_t tfim_mfi_item_total(const tfim_ctx* c) { return c && c->mined ? (int64_t)c->mfis.items.size() : -1; }
 
 int tfim_get_mfis(const tfim_ctx* c, int32_t* items, int64_t* offsets, int32_t* supports) {
     TFIM_CHECK(c && items && offsets && supports, TFIM_E_INVALID, "null argument");
     TFIM_CHECK(c->mined, TFIM_E_STATE, "tfim_get_mfis before tfim_mine");
-    int64_t o = 0;
-    for (size_t k = 0; k < c->mfi_items.size(); k++) {
-        offsets[k] = o;
-        for (int32_t x : c->mfi_items[k]) items[o++] = c->dense_to_orig[x];
-        supports[k] = c->mfi_support[k];
-    }
-    offsets[c->mfi_items.size()] = o;
+    const MfiSet& M = c->mfis;
+    const int32_t* map = c->dense_to_orig.data();
+    for (size_t q = 0; q < M.items.size(); q++) items[q] = map[M.items[q]];
+    std::copy(M.off.begin(), M.off.end(), offsets);
+    std::copy(M.sup.begin(), M.sup.end(), supports);
     return TFIM_OK;
 }
 
@@ -394,12 +391,13 @@ int tfim_write_results(const tfim_ctx* c, const char* trans_set_file, const char
     fprintf(f, "preprocessing_time(s): %g\n", prep_s);
     fprintf(f, "computation_time(s): %g\n", comp_s);
     fprintf(f, "total_time(s): %g\n", prep_s + comp_s);
-    fprintf(f, "\nMFIsNumber: %lld\n", (long long)c->mfi_items.size());
+    fprintf(f, "\nMFIsNumber: %lld\n", (long long)c->mfis.size());
     fprintf(f, "============================List of MFIs:=============================\n");
-    for (size_t k = 0; k < c->mfi_items.size(); k++) {
-        fprintf(f, "%zuth: %zu { ", k + 1, c->mfi_items[k].size());
-        for (int32_t x : c->mfi_items[k]) fprintf(f, "%d ", c->dense_to_orig[x]);
-        fprintf(f, "}   support: %g  frequency: %d\n", (double)c->mfi_support[k] / (double)I.trans_num, c->mfi_support[k]);
+    const MfiSet& M = c->mfis;
+    for (size_t k = 0; k < M.size(); k++) {
+        fprintf(f, "%zuth: %lld { ", k + 1, (long long)(M.off[k + 1] - M.off[k]));
+        for (int64_t q = M.off[k]; q < M.off[k + 1]; q++) fprintf(f, "%d ", c->dense_to_orig[M.items[q]]);
+        fprintf(f, "}   support: %g  frequency: %d\n", (double)M.sup[k] / (double)I.trans_num, M.sup[k]);
     }
     fprintf(f, "==================================================================\n");
     const bool ok = ferror(f) == 0;

@@ -353,8 +353,7 @@ struct MfiSink {
         if (mx < 0 || !is_root[mx]) return;
         std::sort(items.begin(), items.end(), std::greater<int32_t>());
         if (items.size() == 1) sup = c->dense_freq[items[0]];   // a root's own frequency is its F1 count
-        c->mfi_items.push_back(std::move(items));
-        c->mfi_support.push_back(sup);
+        c->mfis.add(items.data(), items.size(), sup);
     }
 };
 
@@ -462,8 +461,7 @@ int run_plain(tfim_ctx* c, const std::vector<int32_t>& roots, WaveRunner& wr, Sl
         if ((size_t)cnt == nd.items.size()) {
             std::vector<int32_t> items = nd.items;
             std::sort(items.begin(), items.end(), std::greater<int32_t>());
-            c->mfi_items.push_back(items);
-            c->mfi_support.push_back(nd.freq);
+            c->mfis.add(items.data(), items.size(), nd.freq);
             continue;
         }
         for (int32_t i = 0; i <= nd.progress - 1; i++) {

@@ -125,10 +125,22 @@ struct ResPtrs {
     int32_t proj_auto;            // let the automatic counter choice pick the projected counter
     Caps caps;
     int64_t row_bytes;            // bytes of one bitmap row (algorithmic traffic accounting)
+    const struct RowSum* row_sum; // first pass of the expand precomputed per wave row (or nullptr)
     // graph-driven wave loop: stop after wave_limit waves or max_launch_ns of device time
     int32_t wave_limit, launch_id;
     unsigned long long max_launch_ns;
 };
+
+// The first pass of the expand over one counted row: extensions (count >= min_count, own
+// column excluded), equal-support extensions, tail extensions, whether an equal-support
+// extension lies outside the tail (the subtree is pruned), and the column blocks of
+// `column_block(nF)` columns that hold an extension.
+struct RowSum {
+    int32_t n_ext, n_eq, n_tail, prune;
+    unsigned long long blocks;
+    int64_t pad;
+};
+__host__ __device__ __forceinline__ int column_block(int nF) { return max(128, (((nF + 63) >> 6) + 31) & ~31); }
 
 // Arguments of the graph-driven wave loop, kept in device memory so that growing a pool
 // only rewrites this record (the captured launches stay valid).
@@ -744,9 +756,13 @@ __device__ void expand_row(const ResPtrs& p, int64_t g, int lane) {
     // later passes read only those.
     bool prune = false;
     int n_ext = 0, n_eq = 0, n_tail = 0;
-    const int bs = max(128, (((nF + 63) >> 6) + 31) & ~31);   // nF / bs <= 64, a multiple of 32
+    const int bs = column_block(nF);   // nF / bs <= 64, a multiple of 32
     unsigned long long blocks = 0;
-    for (int c0 = 0; c0 < nF; c0 += 128) {
+    if (p.row_sum) {
+        const RowSum rs = p.row_sum[g];
+        n_ext = rs.n_ext; n_eq = rs.n_eq; n_tail = rs.n_tail; prune = rs.prune != 0; blocks = rs.blocks;
+    }
+    for (int c0 = 0; c0 < (p.row_sum ? 0 : nF); c0 += 128) {
         int32_t v4[4];
 #pragma unroll
         for (int u = 0; u < 4; u++) {
@@ -1008,6 +1024,54 @@ __global__ void __launch_bounds__(256) k_res_expand(ResPtrs p) {
     expand_row(p, g, threadIdx.x & 31);
 }
 
+// The expand's first pass for the family of the empty prefix (an n x n count block whose
+// rows are its tail, nT = nF = n): one block per row streams the row with four loads in
+// flight per thread and writes the row's summary.
+__global__ void __launch_bounds__(256) k_top_summary(const int32_t* __restrict__ M, int32_t n, int32_t minc,
+                                                     RowSum* __restrict__ out) {
+    const int32_t i = blockIdx.x;
+    const int32_t* row = M + (int64_t)i * n;
+    const int32_t supc = row[i];
+    const int bs = column_block(n);
+    int n_ext = 0, n_eq = 0, n_tail = 0, prune = 0;
+    unsigned long long blocks = 0;
+    for (int c0 = threadIdx.x; c0 < n; c0 += 4 * 256) {
+        int32_t v4[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int c = c0 + u * 256;
+            v4[u] = c < n && c != i ? __ldg(row + c) : -1;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int c = c0 + u * 256;
+            const bool e = v4[u] >= minc;
+            const bool eq = e && v4[u] == supc;
+            const bool in_tail = c > i;
+            n_ext += e;
+            n_eq += eq;
+            n_tail += e && !eq && in_tail;
+            prune |= eq && !in_tail;
+            if (e) blocks |= 1ull << (c / bs);
+        }
+    }
+    typedef cub::BlockReduce<int, 256> RedI;
+    __shared__ typename RedI::TempStorage ti;
+    __shared__ unsigned long long s_blocks;
+    if (threadIdx.x == 0) s_blocks = 0;
+    __syncthreads();
+    if (blocks) atomicOr(&s_blocks, blocks);
+    const int a = RedI(ti).Sum(n_ext);
+    __syncthreads();
+    const int b = RedI(ti).Sum(n_eq);
+    __syncthreads();
+    const int t = RedI(ti).Sum(n_tail);
+    __syncthreads();
+    const int pr = RedI(ti).Reduce(prune, cub::Max());
+    __syncthreads();
+    if (threadIdx.x == 0) out[i] = RowSum{a, b, t, pr, s_blocks, 0};
+}
+
 // ---------------------------------------------------------------------------------- graph loop
 // The wave loop as a graph: a conditional WHILE node whose body is
 //   pack -> zero the count block -> persistent counters -> persistent expand -> control.
@@ -1133,7 +1197,7 @@ int build_wave_graph(WaveGraph& G, const ResArgs* d_args, ResStatus* d_status, b
 struct ResidentState {
     Pool fams, items, heads, stack, looks, free_slots, defer, mfi_off, mfi_len, mfi_sup, mfi_items, log_feat, log_label;
     Pool djobs, jobs, rows, row_job, row_local, tiles_l3, tiles_b1, counts, status, is_root, dense_freq, top_pos, top_diag,
-        proj_list, args;
+        proj_list, args, top_sum;
     HostBuf h_status, h_args;
     WaveGraph graph;
     int32_t launch_id = 0;
@@ -1141,7 +1205,7 @@ struct ResidentState {
         graph.release();
         for (Pool* b : {&fams, &items, &heads, &stack, &looks, &free_slots, &defer, &mfi_off, &mfi_len, &mfi_sup, &mfi_items,
                         &log_feat, &log_label, &djobs, &jobs, &rows, &row_job, &row_local, &tiles_l3, &tiles_b1, &counts,
-                        &status, &is_root, &dense_freq, &top_pos, &top_diag, &proj_list, &args}) {
+                        &status, &is_root, &dense_freq, &top_pos, &top_diag, &proj_list, &args, &top_sum}) {
             dev_free(b->p, s);
             b->p = nullptr;
             b->bytes = 0;
@@ -1330,6 +1394,7 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
         k.log = o->log_lookahead ? (int64_t)std::min(R.log_feat.bytes / 128, R.log_label.bytes / 4) : 0;
         k.rows = cap_rows;
         P.row_bytes = row_bytes;
+        P.row_sum = nullptr;
         P.wave_limit = 0x7fffffff;
         P.launch_id = 0;
         P.max_launch_ns = 2000000000ull;
@@ -1441,10 +1506,15 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
         }
         TFIM_CUDA(cudaEventRecord(c->ev1, s));
         TFIM_TRY(launch_mirror(P.counts, n0, top_mode == 2 ? (const int32_t*)R.top_diag.p : nullptr, s));
-        launches += 2;
+        TFIM_TRY(grow(R.top_sum, (size_t)n0 * sizeof(RowSum), s));
+        k_top_summary<<<n0, 256, 0, s>>>(P.counts, n0, minc, (RowSum*)R.top_sum.p);
+        TFIM_CUDA(cudaGetLastError());
+        launches += 3;
         count_launches++;
         const int64_t threads = (int64_t)n0 * 32;
-        k_res_expand<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(P);
+        ResPtrs Ptop = P;
+        Ptop.row_sum = (const RowSum*)R.top_sum.p;
+        k_res_expand<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(Ptop);
         TFIM_CUDA(cudaGetLastError());
         launches++;
         waves++;
@@ -1563,11 +1633,22 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
         TFIM_CUDA(cudaMemcpyAsync(c->la_labels.data(), R.log_label.p, (size_t)fin.log_n * 4, cudaMemcpyDeviceToHost, s));
     }
     TFIM_CUDA(cudaStreamSynchronize(s));
-    for (int32_t k = 0; k < fin.mfi_n; k++) {
-        std::vector<int32_t> it(mitems.begin() + moff[k], mitems.begin() + moff[k] + mlen[k]);
-        std::sort(it.begin(), it.end(), std::greater<int32_t>());
-        c->mfi_items.push_back(std::move(it));
-        c->mfi_support.push_back(msup[k]);
+    {
+        MfiSet& M = c->mfis;
+        const size_t base = M.items.size();
+        M.items.resize(base + (size_t)fin.mfi_item_n);
+        M.off.reserve(M.off.size() + (size_t)fin.mfi_n);
+        M.sup.reserve(M.sup.size() + (size_t)fin.mfi_n);
+        size_t o = base;
+        for (int32_t k = 0; k < fin.mfi_n; k++) {
+            int32_t* dst = M.items.data() + o;
+            std::copy(mitems.begin() + moff[k], mitems.begin() + moff[k] + mlen[k], dst);
+            std::sort(dst, dst + mlen[k], std::greater<int32_t>());
+            o += (size_t)mlen[k];
+            M.off.push_back((int64_t)o);
+            M.sup.push_back(msup[k]);
+        }
+        M.items.resize(o);
     }
     stt->nodes += (int64_t)fin.nodes;
     stt->supports += (int64_t)fin.supports;

@@ -172,7 +172,28 @@ int launch_compact(const int32_t* counts, const JobDesc* jobs, const int32_t* ro
 
 }  // namespace tfim
 
-namespace tfim { struct EngineState; struct ResidentState; }
+namespace tfim {
+struct EngineState;
+struct ResidentState;
+// The MFIs of a mine, flat: MFI k holds items[off[k] .. off[k+1]) (dense ids, descending)
+// and has support sup[k].
+struct MfiSet {
+    std::vector<int32_t> items;
+    std::vector<int64_t> off{0};
+    std::vector<int32_t> sup;
+    size_t size() const { return sup.size(); }
+    void clear() {
+        items.clear();
+        off.assign(1, 0);
+        sup.clear();
+    }
+    void add(const int32_t* x, size_t n, int32_t s) {
+        items.insert(items.end(), x, x + n);
+        off.push_back((int64_t)items.size());
+        sup.push_back(s);
+    }
+};
+}  // namespace tfim
 
 // ------------------------------------------------------------------ context
 struct tfim_ctx {
@@ -204,8 +225,7 @@ struct tfim_ctx {
     tfim::DevBuf d_masks;                   // mask pool (rows of W words)
     int64_t mask_slots = 0;
     // results
-    std::vector<std::vector<int32_t>> mfi_items;  // dense ids
-    std::vector<int32_t> mfi_support;
+    tfim::MfiSet mfis;                      // dense ids
     bool mined = false;
     int32_t counter_pref = TFIM_COUNTER_AUTO;   // counter used by tfim_count_wave
     tfim_mine_stats last_stats{};

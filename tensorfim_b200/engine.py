@@ -9,7 +9,6 @@ code/engine/src/kernel_bmma.cu:772-872).  ``mine_file`` runs the first through t
 from __future__ import annotations
 
 import ctypes as C
-import dataclasses
 import os
 import subprocess
 
@@ -63,13 +62,40 @@ def read_fimi(path: str) -> tuple[np.ndarray, np.ndarray]:
     return offsets, items
 
 
-@dataclasses.dataclass
 class MineResult:
-    mfis: list            # [(items: tuple of original ids, largest first), support]
-    stats: dict
+    """The MFIs of one mine as flat arrays (``items[offsets[k]:offsets[k+1]]`` are the
+    original ids of MFI k, largest first; ``supports[k]`` its support), in the order
+    tfim_get_mfis returns them.  ``mfis`` builds the list of (items tuple, support) pairs
+    on first use."""
+
+    def __init__(self, items: np.ndarray, offsets: np.ndarray, supports: np.ndarray, stats: dict):
+        self.items, self.offsets, self.supports, self.stats = items, offsets, supports, stats
+        self._mfis = None
+
+    def __len__(self) -> int:
+        return int(self.supports.shape[0])
+
+    @property
+    def mfis(self) -> list:
+        if self._mfis is None:
+            it, off = self.items.tolist(), self.offsets.tolist()
+            self._mfis = [(tuple(it[off[k]:off[k + 1]]), s) for k, s in enumerate(self.supports.tolist())]
+        return self._mfis
 
     def as_dict(self) -> dict:
         return {frozenset(items): sup for items, sup in self.mfis}
+
+
+_SHIPPED = {}
+
+
+def shipped_proposal(device: int = 0):
+    """The trained proposal network shipped with the package, loaded once per device and
+    shared by every Database on that device (a context does not own its proposal)."""
+    if device not in _SHIPPED:
+        from .learn import Proposal
+        _SHIPPED[device] = Proposal.load(device=device)
+    return _SHIPPED[device]
 
 
 class Database:
@@ -170,8 +196,7 @@ class Database:
         o.counter = COUNTERS[counter]
         la = {False: 0, True: 1, "off": 0, "filtered": 1, "learned": 2, "all": 3}[lookahead]
         if la == 2 and getattr(self, "_proposal", None) is None:
-            from .learn import Proposal
-            self.set_proposal(Proposal.load(device=self._device))
+            self.set_proposal(shipped_proposal(self._device))
         o.lookahead = la
         o.log_lookahead = int(log_lookahead)
         o.proj_auto = int(proj_auto)
@@ -187,8 +212,7 @@ class Database:
         offs = np.zeros(n + 1, dtype=np.int64)
         sup = np.zeros(max(n, 1), dtype=np.int32)
         check(lib().tfim_get_mfis(self._h, _ptr(items), _ptr(offs), _ptr(sup)))
-        mfis = [(tuple(int(x) for x in items[offs[k]:offs[k + 1]]), int(sup[k])) for k in range(n)]
-        return MineResult(mfis, st.as_dict())
+        return MineResult(items[:tot], offs, sup[:n], st.as_dict())
 
     def write_results(self, trans_set_file: str, result_path: str, prep_s: float = 0.0, comp_s: float = 0.0) -> None:
         check(lib().tfim_write_results(self._h, trans_set_file.encode(), result_path.encode(), prep_s, comp_s))
