@@ -118,8 +118,9 @@ def make_db(name: str):
 def run_reference_arm(args, rank: int, world: int) -> int:
     """The reference's own CPU implementation (oracle/_ref/tfim_ref_mt: code/engine/src/
     kernel_bitmap.cu compiled unmodified, RUN_MODE 2 with every node on its multithreaded
-    CPU counter), on a bounded sample of the workload: the same generator at 5% of the rows
-    and the same minimum support.  Its per-support cost is linear in the transaction count,
+    CPU counter), on a bounded sample of the workload: the same generator at --ref-scale of
+    the rows (default 2%) and the same minimum support.  Under torchrun only rank 0 runs it;
+    the other ranks exit 0 without work.  Its per-support cost is linear in the transaction count,
     so supports are scaled by N_sample/N_full to full-workload supports."""
     if rank != 0:
         return 0
@@ -192,6 +193,7 @@ def main() -> int:
     import torch
     import torch.distributed as dist
     import tensorfim_b200 as tf
+    from tensorfim_b200 import replicas
 
     torch.cuda.set_device(local)
     if world > 1:
@@ -204,11 +206,7 @@ def main() -> int:
         torch.cuda.synchronize()
 
     def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.max_over_ranks(x, device="cuda")
 
     db0, w = make_db(args.workload)
     # pinned host copies of the inputs (the e2e path copies them every step)
@@ -248,7 +246,7 @@ def main() -> int:
     else:
         ref_supports = batched.stats["supports"]
         identical = None
-    value = world * ref_supports / (ms / 1000.0)
+    value = replicas.job_throughput(ref_supports, ms, world)
 
     # end to end through the C ABI from pinned host memory
     e2e = None
@@ -267,7 +265,7 @@ def main() -> int:
                 e2e_ms.append((t1 - t0) * 1000.0)
             d2h = res.items.nbytes + res.offsets.nbytes + res.supports.nbytes
         e2e_t = max_over_ranks(statistics.mean(e2e_ms))
-        e2e = {"value": world * ref_supports / (e2e_t / 1000.0), "unit": "supports/s", "h2d_bytes_per_step": int(h2d_bytes),
+        e2e = {"value": replicas.job_throughput(ref_supports, e2e_t, world), "unit": "supports/s", "h2d_bytes_per_step": int(h2d_bytes),
                "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_t,
                "timing": "host wall clock around open (H2D + device ingest) + mine + MFI read-back + close"}
 
