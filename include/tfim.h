@@ -195,8 +195,39 @@ typedef struct {
     double  host_ms;           /* host time spent building waves and processing results */
     double  sync_ms;           /* host time blocked on device results */
     int64_t lookaheads_skipped;/* lookaheads ruled out because a tail pair is infrequent */
-    int64_t reserved[1];
+    double  top_ms;            /* CUDA-event time of counting the empty-prefix family (resident) */
 } tfim_mine_stats;
+
+/* ------------------------------------------------------------------ tuning table
+ * Launch shapes and counter selection of the engines.  The reference fixes these as
+ * constants (wave cap clamp(96 MiB / row bytes, 64, 1024) and split-k <= 32 in
+ * code/engine/src/kernel_bmma.cu:636-768,896-910; no selection between counters); here
+ * they form a table whose built-in values were measured on B200 and which
+ * `python -m tensorfim_b200.autotune` re-measures by sweeping the benchmark databases and
+ * writes to tensorfim_b200/tuning.json.  The library loads that file (the `tuning.json`
+ * in the parent directory of libtfim.so) the first time a tuning value is needed.
+ * Set or load a table before mining; a mine in flight reads the table once at its start. */
+typedef struct {
+    int32_t wave_rows;          /* family rows per wave (resident and batched engines) */
+    float   l3_slices_per_sm;   /* CUDA-core work split: tile slices per SM and wave */
+    float   b1_tiles_per_sm;    /* tensor-core split-k target: tiles per SM and wave */
+    int32_t b1_min_rows;        /* automatic counter choice: the tensor path for count jobs */
+    int32_t b1_min_cols;        /*   of at least b1_min_rows rows x b1_min_cols columns */
+    int32_t proj_auto;          /* automatic choice may pick the projected counter (0/1) */
+    double  rate_b1_bitops;     /* cost model of the empty-prefix family: b1 bit-ops/s, */
+    double  rate_lop3_bitops;   /*   LOP3 bit-ops/s, */
+    double  rate_pair_incr;     /*   pair co-occurrence increments/s */
+    int32_t reserved[8];
+} tfim_tuning;
+
+/* The table in force (built-in values, or the loaded / set table). */
+TFIM_API void tfim_tuning_get(tfim_tuning* out);
+/* Replace the table; values out of range give TFIM_E_INVALID and change nothing. */
+TFIM_API int tfim_tuning_set(const tfim_tuning* t);
+/* Load a flat JSON object {"wave_rows": 4096, ...}; keys not given keep their value. */
+TFIM_API int tfim_tuning_load(const char* path);
+/* "built-in" or the path of the table loaded last. */
+TFIM_API const char* tfim_tuning_source(void);
 
 TFIM_API void tfim_mine_opts_default(tfim_mine_opts* opts);
 

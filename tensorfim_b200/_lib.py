@@ -38,6 +38,7 @@ EXPORTS = [
     "tfim_count_wave_noalloc",
     "tfim_mlp_create", "tfim_mlp_num_params", "tfim_mlp_set_params", "tfim_mlp_get_params", "tfim_mlp_predict",
     "tfim_mlp_grad", "tfim_mlp_train", "tfim_mlp_free", "tfim_set_proposal", "tfim_lookahead_log",
+    "tfim_tuning_get", "tfim_tuning_set", "tfim_tuning_load", "tfim_tuning_source",
 ]
 
 
@@ -69,13 +70,23 @@ class MineOpts(C.Structure):
                 ("reserved", C.c_int32 * 7)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("wave_rows", C.c_int32), ("l3_slices_per_sm", C.c_float), ("b1_tiles_per_sm", C.c_float),
+                ("b1_min_rows", C.c_int32), ("b1_min_cols", C.c_int32), ("proj_auto", C.c_int32),
+                ("rate_b1_bitops", C.c_double), ("rate_lop3_bitops", C.c_double), ("rate_pair_incr", C.c_double),
+                ("reserved", C.c_int32 * 8)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
 class MineStats(C.Structure):
     _fields_ = [("mine_seconds", C.c_double), ("device_ms", C.c_double), ("kernel_ms", C.c_double),
                 ("nodes", C.c_int64), ("supports", C.c_int64), ("bit_ops", C.c_int64), ("bytes_alg", C.c_int64),
                 ("waves", C.c_int64), ("launches", C.c_int64), ("count_launches", C.c_int64),
                 ("lookaheads", C.c_int64), ("lookahead_hits", C.c_int64), ("pruned_pep", C.c_int64),
                 ("n_mfi", C.c_int64), ("host_ms", C.c_double), ("sync_ms", C.c_double),
-                ("lookaheads_skipped", C.c_int64), ("reserved", C.c_int64 * 1)]
+                ("lookaheads_skipped", C.c_int64), ("top_ms", C.c_double)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
@@ -128,6 +139,11 @@ def lib() -> C.CDLL:
     L.tfim_set_proposal.argtypes = [p, p, C.c_float]
     L.tfim_lookahead_log.argtypes = [p, p, p, i64]
     L.tfim_lookahead_log.restype = i64
+    L.tfim_tuning_get.argtypes = [P(Tuning)]
+    L.tfim_tuning_get.restype = None
+    L.tfim_tuning_set.argtypes = [P(Tuning)]
+    L.tfim_tuning_load.argtypes = [C.c_char_p]
+    L.tfim_tuning_source.restype = C.c_char_p
     for name in EXPORTS:
         getattr(L, name)   # raises AttributeError if an export is missing
     _lib = L

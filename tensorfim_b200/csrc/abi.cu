@@ -54,7 +54,8 @@ int count_wave_impl(tfim_ctx* c, int32_t b, int32_t min_count, const int32_t* d_
     if (d == 0) return launch_nfreq(d_counts, b, 0, min_count, d_nfreq, s);
     // host-built job/tile tables (independent of the list contents)
     const int32_t counter = c->counter_pref;
-    const bool b1 = counter == TFIM_COUNTER_TENSOR || (counter == TFIM_COUNTER_AUTO && b >= 16 && d >= 16);
+    const tfim_tuning tn = tuning();
+    const bool b1 = counter == TFIM_COUNTER_TENSOR || (counter == TFIM_COUNTER_AUTO && b >= tn.b1_min_rows && d >= tn.b1_min_cols);
     std::vector<JobDesc> jobs(1);
     jobs[0].base_slot = -1; jobs[0].base_item = -1;
     jobs[0].n_rows = b; jobs[0].n_cols = d; jobs[0].row_off = 0; jobs[0].col_off = 0; jobs[0].out_off = 0;
@@ -67,7 +68,8 @@ int count_wave_impl(tfim_ctx* c, int32_t b, int32_t min_count, const int32_t* d_
     const int64_t W = c->W;
     if (b1) {
         const int64_t base = (int64_t)((b + kB1Rows - 1) / kB1Rows) * ((d + kB1Cols - 1) / kB1Cols);
-        int64_t ks = std::max<int64_t>(1, (4LL * 148 + base - 1) / base);
+        const int64_t want = (int64_t)(tn.b1_tiles_per_sm * 148);
+        int64_t ks = std::max<int64_t>(1, (want + base - 1) / base);
         ks = std::min<int64_t>(ks, W / 64);
         const int64_t kslice = ((W / 64 + ks - 1) / ks) * 64;
         for (int64_t w0 = 0; w0 < W; w0 += kslice)

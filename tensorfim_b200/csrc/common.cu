@@ -1,5 +1,8 @@
 // Error state, buffers and small helpers shared by the engine.
+#include <dlfcn.h>
+
 #include <cstdarg>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -128,9 +131,129 @@ void HostBuf::release() {
     bytes = 0;
 }
 
+// ------------------------------------------------------------------ tuning table
+namespace {
+std::mutex g_tune_mu;
+bool g_tune_init = false;
+tfim_tuning g_tune;
+std::string g_tune_src = "built-in";
+
+void tuning_builtin(tfim_tuning* t) {
+    memset(t, 0, sizeof *t);
+    t->wave_rows = 4096;
+    t->l3_slices_per_sm = 8.f;
+    t->b1_tiles_per_sm = 4.f;
+    t->b1_min_rows = 16;
+    t->b1_min_cols = 16;
+    t->proj_auto = kTuneProjAuto;
+    t->rate_b1_bitops = kTuneB1BitOps;
+    t->rate_lop3_bitops = kTuneLop3BitOps;
+    t->rate_pair_incr = kTunePairIncrements;
+}
+
+bool tuning_valid(const tfim_tuning& t) {
+    return t.wave_rows >= 16 && t.wave_rows <= (1 << 20) && t.l3_slices_per_sm > 0.f && t.l3_slices_per_sm <= 1024.f &&
+           t.b1_tiles_per_sm > 0.f && t.b1_tiles_per_sm <= 1024.f && t.b1_min_rows >= 1 && t.b1_min_cols >= 1 &&
+           (t.proj_auto == 0 || t.proj_auto == 1) && t.rate_b1_bitops > 0 && t.rate_lop3_bitops > 0 && t.rate_pair_incr > 0;
+}
+
+// Flat JSON object of numbers: {"key": value, ...}.  Unknown keys are ignored.
+int tuning_parse(const std::string& text, tfim_tuning* t) {
+    struct Key { const char* name; int kind; void* dst; };   // kind 0 int, 1 float, 2 double
+    const Key keys[] = {{"wave_rows", 0, &t->wave_rows},       {"l3_slices_per_sm", 1, &t->l3_slices_per_sm},
+                        {"b1_tiles_per_sm", 1, &t->b1_tiles_per_sm}, {"b1_min_rows", 0, &t->b1_min_rows},
+                        {"b1_min_cols", 0, &t->b1_min_cols},   {"proj_auto", 0, &t->proj_auto},
+                        {"rate_b1_bitops", 2, &t->rate_b1_bitops}, {"rate_lop3_bitops", 2, &t->rate_lop3_bitops},
+                        {"rate_pair_incr", 2, &t->rate_pair_incr}};
+    for (const Key& k : keys) {
+        const std::string pat = std::string("\"") + k.name + "\"";
+        const size_t at = text.find(pat);
+        if (at == std::string::npos) continue;
+        size_t colon = text.find(':', at + pat.size());
+        if (colon == std::string::npos) return TFIM_E_INVALID;
+        const char* b = text.c_str() + colon + 1;
+        char* e = nullptr;
+        const double v = strtod(b, &e);
+        if (e == b) return TFIM_E_INVALID;
+        if (k.kind == 0) *(int32_t*)k.dst = (int32_t)v;
+        else if (k.kind == 1) *(float*)k.dst = (float)v;
+        else *(double*)k.dst = v;
+    }
+    return TFIM_OK;
+}
+
+int tuning_load_locked(const char* path) {
+    FILE* f = fopen(path, "rb");
+    TFIM_CHECK(f, TFIM_E_IO, "cannot open tuning table %s", path);
+    std::string text;
+    char buf[4096];
+    size_t n;
+    while ((n = fread(buf, 1, sizeof buf, f)) > 0) text.append(buf, n);
+    fclose(f);
+    tfim_tuning t = g_tune;
+    TFIM_CHECK(tuning_parse(text, &t) == TFIM_OK, TFIM_E_INVALID, "malformed tuning table %s", path);
+    TFIM_CHECK(tuning_valid(t), TFIM_E_INVALID, "tuning table %s holds a value out of range", path);
+    g_tune = t;
+    g_tune_src = path;
+    return TFIM_OK;
+}
+
+// First use: built-in values, then the table shipped beside the library if present.
+void tuning_init_locked() {
+    if (g_tune_init) return;
+    g_tune_init = true;
+    tuning_builtin(&g_tune);
+    Dl_info info;
+    if (dladdr((const void*)&tuning_builtin, &info) && info.dli_fname) {
+        std::string so = info.dli_fname;
+        const size_t slash = so.rfind('/');
+        const std::string dir = slash == std::string::npos ? std::string(".") : so.substr(0, slash);
+        const std::string path = dir + "/../tuning.json";
+        FILE* f = fopen(path.c_str(), "rb");
+        if (f) {
+            fclose(f);
+            tuning_load_locked(path.c_str());   // a bad table leaves the built-in values
+        }
+    }
+}
+}  // namespace
+
+tfim_tuning tuning() {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    tuning_init_locked();
+    return g_tune;
+}
+
 }  // namespace tfim
 
 extern "C" {
+
+void tfim_tuning_get(tfim_tuning* out) {
+    if (out) *out = tfim::tuning();
+}
+
+int tfim_tuning_set(const tfim_tuning* t) {
+    TFIM_CHECK(t, TFIM_E_INVALID, "null tuning table");
+    TFIM_CHECK(tfim::tuning_valid(*t), TFIM_E_INVALID, "tuning value out of range");
+    std::lock_guard<std::mutex> lk(tfim::g_tune_mu);
+    tfim::tuning_init_locked();
+    tfim::g_tune = *t;
+    tfim::g_tune_src = "set by the caller";
+    return TFIM_OK;
+}
+
+int tfim_tuning_load(const char* path) {
+    TFIM_CHECK(path, TFIM_E_INVALID, "null path");
+    std::lock_guard<std::mutex> lk(tfim::g_tune_mu);
+    tfim::tuning_init_locked();
+    return tfim::tuning_load_locked(path);
+}
+
+const char* tfim_tuning_source(void) {
+    std::lock_guard<std::mutex> lk(tfim::g_tune_mu);
+    tfim::tuning_init_locked();
+    return tfim::g_tune_src.c_str();
+}
 
 const char* tfim_version(void) { return "tensorfim-b200 0.1 (sm_100a)"; }
 const char* tfim_last_error(void) { return tfim::get_error(); }

@@ -191,6 +191,7 @@ struct WaveRunner {
 
     int run(Wave& w, int32_t min_count, bool want_full_counts, std::vector<int32_t>* full_counts) {
         const int64_t W = c->W;
+        const tfim_tuning tn = tuning();
         std::vector<TileDesc> t_l3, t_b1;
         // split-k factor for tensor tiles: enough tiles to cover the SMs a few times
         int64_t base_b1 = 0;
@@ -204,14 +205,14 @@ struct WaveRunner {
                 base_l3 += (int64_t)((w.jobs[j].n_rows + kLop3Rows - 1) / kLop3Rows) * ((w.jobs[j].n_cols + 63) / 64);
         int64_t wslice = W;
         if (base_l3 > 0) {
-            const int64_t want = 8LL * sm_count;
+            const int64_t want = (int64_t)(tn.l3_slices_per_sm * sm_count);
             int64_t ks = std::max<int64_t>(1, (want + base_l3 - 1) / base_l3);
             ks = std::min<int64_t>(ks, std::max<int64_t>(1, W / 256));
             wslice = ((W / 64 + ks - 1) / ks) * 64;
         }
         int64_t kslice = W;
         if (base_b1 > 0) {
-            const int64_t want = 4LL * sm_count;
+            const int64_t want = (int64_t)(tn.b1_tiles_per_sm * sm_count);
             int64_t ks = std::max<int64_t>(1, (want + base_b1 - 1) / base_b1);
             ks = std::min<int64_t>(ks, W / 64);
             kslice = ((W / 64 + ks - 1) / ks) * 64;
@@ -566,7 +567,8 @@ int mine_batched(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* st) {
     std::deque<Fam> fams;   // stable references while children are appended
     std::vector<int32_t> stack;             // family ids, top = back
     std::vector<Look> looks_pending;        // issued with the next wave
-    const int32_t wave_cap = o->wave_cap > 0 ? o->wave_cap : 4096;
+    const tfim_tuning tn = tuning();
+    const int32_t wave_cap = o->wave_cap > 0 ? o->wave_cap : tn.wave_rows;
     const int32_t la_mode = o->lookahead;   // 0 off, 1 filtered, 2 learned, 3 every node
     const bool lookahead = la_mode != 0;
     TFIM_CHECK(la_mode != 2 || c->proposal, TFIM_E_STATE, "lookahead mode 2 needs a proposal network (tfim_set_proposal)");
@@ -588,10 +590,11 @@ int mine_batched(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* st) {
     if (!fams.empty()) {
         const double nF = (double)fams[0].F.size();
         const bool fits = nF * nF * 4.0 <= (double)(1LL << 32);
-        const bool b1 = wr.counter != TFIM_COUNTER_LOP3 && (wr.counter == TFIM_COUNTER_TENSOR || nF >= 16);
-        const double bit_rate = b1 ? kTuneB1BitOps : kTuneLop3BitOps;
+        const bool b1 = wr.counter != TFIM_COUNTER_LOP3 &&
+                        (wr.counter == TFIM_COUNTER_TENSOR || (nF >= tn.b1_min_rows && nF >= tn.b1_min_cols));
+        const double bit_rate = b1 ? tn.rate_b1_bitops : tn.rate_lop3_bitops;
         const double bitmap_s = nF * nF * (double)c->n_bits / 2.0 / bit_rate;
-        const double pairs_s = c->red_pair_work / 2.0 / kTunePairIncrements + nF * nF * 4.0 / kTuneHbmBytes;
+        const double pairs_s = c->red_pair_work / 2.0 / tn.rate_pair_incr + nF * nF * 4.0 / kTuneHbmBytes;
         if (fits) {
             if (o->top_counter == 1) top_mode = 1;
             else if (o->top_counter == 2) top_mode = c->csr_exact ? 2 : 1;
@@ -601,7 +604,7 @@ int mine_batched(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* st) {
     auto use_b1_for = [&](int32_t nr, int32_t nc) {
         if (wr.counter == TFIM_COUNTER_LOP3) return false;
         if (wr.counter == TFIM_COUNTER_TENSOR) return true;
-        return nr >= 16 && nc >= 16;
+        return nr >= tn.b1_min_rows && nc >= tn.b1_min_cols;
     };
 
     Wave w;
@@ -815,9 +818,7 @@ int mine_batched(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* st) {
             if (la_mode == 2) {
                 std::vector<float> feats(cands.size() * 32);
                 for (size_t q = 0; q < cands.size(); q++) memcpy(&feats[q * 32], cands[q].feat, 32 * sizeof(float));
-                const double tp = now_s();
                 if (tfim_mlp_predict(c->proposal, feats.data(), (int64_t)cands.size(), probs.data()) != TFIM_OK) return TFIM_E_CUDA;
-                st->reserved[0] += (int64_t)((now_s() - tp) * 1e6);   // proposal time, microseconds
             }
             for (size_t q = 0; q < cands.size(); q++) {
                 const Cand& cd = cands[q];

@@ -123,6 +123,8 @@ struct ResPtrs {
     float avg_len;                // mean reduced transaction length
     int32_t csr_ok;               // the reduced transaction list repeats no id within a row
     int32_t proj_auto;            // let the automatic counter choice pick the projected counter
+    int32_t b1_min_rows, b1_min_cols;   // automatic choice: tensor path from this job shape
+    float l3_slices_per_sm, b1_tiles_per_sm;   // work split targets per wave
     Caps caps;
     int64_t row_bytes;            // bytes of one bitmap row (algorithmic traffic accounting)
     const struct RowSum* row_sum; // first pass of the expand precomputed per wave row (or nullptr)
@@ -178,7 +180,7 @@ constexpr int kPackCand = kPackThreads * kPackItems;
 __device__ __forceinline__ bool use_b1_shape(const ResPtrs& p, int nr, int nc) {
     if (p.counter == TFIM_COUNTER_LOP3) return false;
     if (p.counter == TFIM_COUNTER_TENSOR) return true;
-    return nr >= 16 && nc >= 16;
+    return nr >= p.b1_min_rows && nc >= p.b1_min_cols;
 }
 __device__ __forceinline__ int64_t l3_tiles(int nr, int nc) { return (int64_t)((nr + kLop3Rows - 1) / kLop3Rows) * ((nc + 63) / 64); }
 __device__ __forceinline__ int64_t b1_tiles(int nr, int nc) { return (int64_t)((nr + kB1Rows - 1) / kB1Rows) * ((nc + kB1Cols - 1) / kB1Cols); }
@@ -469,7 +471,7 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
         __syncthreads();
     }
     // about 8 tile slices per SM: two rounds of the 4 resident blocks
-    const float target = fmaxf(s_cost / (8.f * (float)p.sm_count), 1.f);
+    const float target = fmaxf(s_cost / (p.l3_slices_per_sm * (float)p.sm_count), 1.f);
     const int64_t max_sl = lmax(1, W / 256);
     int64_t tot3 = 0;
     for (int base = 0; base < nj; base += kPackCand) {
@@ -499,7 +501,8 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
         tot3 += g3;
         __syncthreads();
     }
-    int64_t ks1 = tot1 > 0 ? lmax(1, (4LL * p.sm_count + tot1 - 1) / tot1) : 1;
+    const int64_t want1 = lmax(1, (int64_t)(p.b1_tiles_per_sm * (float)p.sm_count));
+    int64_t ks1 = tot1 > 0 ? lmax(1, (want1 + tot1 - 1) / tot1) : 1;
     ks1 = lmin(ks1, lmax(1, W / 64));
     int64_t kslice = ((W / 64 + ks1 - 1) / ks1) * 64;
     if (kslice <= 0) kslice = 64;
@@ -1252,7 +1255,8 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, dev);
     }
-    const int32_t wave_rows = o->wave_cap > 0 ? o->wave_cap : 4096;
+    const tfim_tuning tn = tuning();
+    const int32_t wave_rows = o->wave_cap > 0 ? o->wave_cap : tn.wave_rows;
     const int64_t top_out = (int64_t)n0 * n0;
     const bool small = o->small_pools != 0;
     const size_t gmin = small ? 64 : (1 << 16);
@@ -1342,14 +1346,16 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
     int top_mode;
     {
         const double nF = n0;
-        const bool b1 = o->counter != TFIM_COUNTER_LOP3 && (o->counter == TFIM_COUNTER_TENSOR || nF >= 16);
-        const double bitmap_s = nF * nF * (double)c->n_bits / 2.0 / (b1 ? kTuneB1BitOps : kTuneLop3BitOps);
-        const double pairs_s = c->red_pair_work / 2.0 / kTunePairIncrements + nF * nF * 4.0 / kTuneHbmBytes;
+        const bool b1 = o->counter != TFIM_COUNTER_LOP3 &&
+                        (o->counter == TFIM_COUNTER_TENSOR || (nF >= tn.b1_min_rows && nF >= tn.b1_min_cols));
+        const double bitmap_s = nF * nF * (double)c->n_bits / 2.0 / (b1 ? tn.rate_b1_bitops : tn.rate_lop3_bitops);
+        const double pairs_s = c->red_pair_work / 2.0 / tn.rate_pair_incr + nF * nF * 4.0 / kTuneHbmBytes;
         if (o->top_counter == 1) top_mode = 1;
         else if (o->top_counter == 2) top_mode = c->csr_exact ? 2 : 1;
         else top_mode = (c->csr_exact && pairs_s < bitmap_s) ? 2 : 1;
     }
-    const bool top_b1 = o->counter == TFIM_COUNTER_TENSOR || (o->counter != TFIM_COUNTER_LOP3 && n0 >= 16);
+    const bool top_b1 = o->counter == TFIM_COUNTER_TENSOR ||
+                        (o->counter != TFIM_COUNTER_LOP3 && n0 >= tn.b1_min_rows && n0 >= tn.b1_min_cols);
 
     const double t_host0 = std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
     double sync_ms = 0, kernel_ms = 0;
@@ -1375,7 +1381,11 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
         P.proj_list = (int32_t*)R.proj_list.p;
         P.avg_len = c->n_bits > 0 ? (float)((double)c->n_red_items / (double)c->n_bits) : 0.f;
         P.csr_ok = c->csr_exact ? 1 : 0;
-        P.proj_auto = o->proj_auto >= 0 ? o->proj_auto : kTuneProjAuto;
+        P.proj_auto = o->proj_auto >= 0 ? o->proj_auto : tn.proj_auto;
+        P.b1_min_rows = tn.b1_min_rows;
+        P.b1_min_cols = tn.b1_min_cols;
+        P.l3_slices_per_sm = tn.l3_slices_per_sm;
+        P.b1_tiles_per_sm = tn.b1_tiles_per_sm;
         if (la_mode == 2 && c->proposal) {
             const void* wb = nullptr;
             const float* pp = nullptr;
@@ -1471,12 +1481,14 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
         if (top_mode == 1) {
             if (top_b1) {
                 const int64_t base = (int64_t)((n0 + kB1Rows - 1) / kB1Rows) * ((n0 + kB1Cols - 1) / kB1Cols);
-                int64_t ks = std::min<int64_t>(std::max<int64_t>(1, (4LL * sm_count + base - 1) / base), W / 64);
+                const int64_t want = (int64_t)(tn.b1_tiles_per_sm * sm_count);
+                int64_t ks = std::min<int64_t>(std::max<int64_t>(1, (want + base - 1) / base), W / 64);
                 const int64_t kslice = ((W / 64 + ks - 1) / ks) * 64;
                 tiles_b1(0, n0, n0, W, kslice, tl, true);
             } else {
                 const int64_t base = (int64_t)((n0 + kLop3Rows - 1) / kLop3Rows) * ((n0 + 63) / 64);
-                int64_t ws = std::min<int64_t>(std::max<int64_t>(1, (8LL * sm_count + base - 1) / base), std::max<int64_t>(1, W / 256));
+                const int64_t want = (int64_t)(tn.l3_slices_per_sm * sm_count);
+                int64_t ws = std::min<int64_t>(std::max<int64_t>(1, (want + base - 1) / base), std::max<int64_t>(1, W / 256));
                 const int64_t wslice = ((W / 64 + ws - 1) / ws) * 64;
                 tiles_lop3(0, n0, n0, W, wslice, tl, true);
             }
@@ -1522,6 +1534,7 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
         TFIM_CUDA(cudaEventSynchronize(c->ev1));
         cudaEventElapsedTime(&ms, c->ev0, c->ev1);
         kernel_ms += ms;
+        stt->top_ms += ms;
     }
     // following waves
     const bool use_graph = o->use_graphs != 0;

@@ -151,6 +151,8 @@ int launch_count_proj_persistent(const CountArgs* d_args, const int32_t* d_n_job
 // blocks of each persistent kernel resident per SM
 int persistent_occupancy(int* lop3, int* b1, int* proj);
 int configure_count_kernels();
+// The tuning table in force (common.cu): built-in values, or the table loaded / set.
+tfim_tuning tuning();
 int launch_pair_count(const int64_t* red_off, const int32_t* red_items, int64_t n_red, const int32_t* pos,
                       int32_t nF, int32_t* M, cudaStream_t s);
 int launch_mirror(int32_t* M, int32_t nF, const int32_t* diag, cudaStream_t s);

@@ -86,6 +86,32 @@ class MineResult:
         return {frozenset(items): sup for items, sup in self.mfis}
 
 
+def tuning() -> dict:
+    """The tuning table in force (include/tfim.h tfim_tuning)."""
+    t = _lib.Tuning()
+    lib().tfim_tuning_get(C.byref(t))
+    return t.as_dict()
+
+
+def set_tuning(**values) -> None:
+    """Replace entries of the tuning table, e.g. set_tuning(wave_rows=2048)."""
+    t = _lib.Tuning()
+    lib().tfim_tuning_get(C.byref(t))
+    for k, v in values.items():
+        if k not in t.as_dict():
+            raise KeyError(k)
+        setattr(t, k, v)
+    check(lib().tfim_tuning_set(C.byref(t)))
+
+
+def load_tuning(path: str) -> None:
+    check(lib().tfim_tuning_load(path.encode()))
+
+
+def tuning_source() -> str:
+    return lib().tfim_tuning_source().decode()
+
+
 _SHIPPED = {}
 
 
@@ -155,6 +181,10 @@ class Database:
         check(lib().tfim_set_counter(self._h, COUNTERS[counter]))
         check(lib().tfim_count_wave(self._h, _ptr(flat), _ptr(offs), b, int(min_count), _ptr(counts), _ptr(nfreq)))
         return counts, nfreq
+
+    def set_counter(self, counter: str) -> None:
+        """Counter used by count_wave / count_wave_device: auto, lop3, tensor."""
+        check(lib().tfim_set_counter(self._h, COUNTERS[counter]))
 
     def count_wave_device(self, d_items: int, d_offsets: int, b: int, max_len: int, min_count: int,
                           d_counts: int, d_nfreq: int, stream: int = 0) -> None:

@@ -150,3 +150,24 @@ def test_cfg3_replicated_matches_base_scaled():
         b = db.mine().as_dict()
     assert b == {k: v * 64 for k, v in a.items()}
     assert len(a) > 10
+
+
+@pytest.mark.parametrize("name", ["cfg1_full", "cfg4_s001", "cfg5_s002", "edge_ties", "cfg3_base"])
+def test_any_tuning_keeps_output(tmp_path, name):
+    """The tuning table changes launch shapes and counter choices, never the MFI set."""
+    from tensorfim_b200 import engine
+    fx = load_golden(name)
+    path = golden_input(fx, tmp_path)
+    saved = engine.tuning()
+    try:
+        with tf.Database.from_file(path, fx["spec"]["minsup"]) as db:
+            for t in (dict(wave_rows=16, l3_slices_per_sm=64.0, b1_tiles_per_sm=32.0, b1_min_rows=2, b1_min_cols=2),
+                      dict(wave_rows=65536, l3_slices_per_sm=1.0, b1_tiles_per_sm=1.0, b1_min_rows=512,
+                           b1_min_cols=512, rate_pair_incr=1e6)):
+                engine.set_tuning(**t)
+                for eng in ("resident", "batched"):
+                    assert db.mine(engine=eng).as_dict() == fx["expected"], (t, eng)
+                assert db.mine(engine="resident", graphs=True).as_dict() == fx["expected"], t
+    finally:
+        engine.set_tuning(**saved)
+
