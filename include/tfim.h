@@ -44,6 +44,8 @@ typedef struct tfim_ctx tfim_ctx;
 #define TFIM_COUNTER_AUTO    0   /* chosen per job from its shape */
 #define TFIM_COUNTER_LOP3    1   /* AND + popc on CUDA cores */
 #define TFIM_COUNTER_TENSOR  2   /* b1 AND+POPC tensor-core MMA */
+#define TFIM_COUNTER_I8      4   /* tcgen05.mma kind::i8 on the bits expanded to bytes
+                                    (tfim_count_wave only) */
 #define TFIM_COUNTER_PROJ    3   /* resident engine: projected counting (prefix transactions x
                                     the reduced transaction list) wherever it applies, else auto */
 
@@ -117,7 +119,7 @@ TFIM_API int tfim_dense_freq(const tfim_ctx* ctx, int32_t* out);
 TFIM_API int tfim_count_wave(tfim_ctx* ctx, const int32_t* item_lists, const int64_t* list_offsets,
                     int32_t b, int32_t min_count, int32_t* counts_out, int32_t* nfreq_out);
 
-/* Choose the counter tfim_count_wave uses: TFIM_COUNTER_AUTO (default), _LOP3 or _TENSOR. */
+/* Choose the counter tfim_count_wave uses: TFIM_COUNTER_AUTO (default), _LOP3, _TENSOR or _I8. */
 TFIM_API int tfim_set_counter(tfim_ctx* ctx, int32_t counter);
 
 /*
@@ -217,7 +219,11 @@ typedef struct {
     double  rate_b1_bitops;     /* cost model of the empty-prefix family: b1 bit-ops/s, */
     double  rate_lop3_bitops;   /*   LOP3 bit-ops/s, */
     double  rate_pair_incr;     /*   pair co-occurrence increments/s */
-    int32_t reserved[8];
+    int32_t i8_min_rows;        /* automatic choice: the tcgen05 kind::i8 counter for count jobs */
+    int32_t i8_min_cols;        /*   of at least i8_min_rows x i8_min_cols (tfim_count_wave and
+                                     the empty-prefix family's bitmap Gram) */
+    double  rate_i8_bitops;     /* cost model: tcgen05 kind::i8 bit-ops/s */
+    int32_t reserved[4];
 } tfim_tuning;
 
 /* The table in force (built-in values, or the loaded / set table). */

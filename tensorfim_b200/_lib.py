@@ -28,6 +28,7 @@ COUNTER_AUTO = 0
 COUNTER_LOP3 = 1
 COUNTER_TENSOR = 2
 COUNTER_PROJ = 3
+COUNTER_I8 = 4
 
 # every entry point declared in include/tfim.h
 EXPORTS = [
@@ -74,7 +75,8 @@ class Tuning(C.Structure):
     _fields_ = [("wave_rows", C.c_int32), ("l3_slices_per_sm", C.c_float), ("b1_tiles_per_sm", C.c_float),
                 ("b1_min_rows", C.c_int32), ("b1_min_cols", C.c_int32), ("proj_auto", C.c_int32),
                 ("rate_b1_bitops", C.c_double), ("rate_lop3_bitops", C.c_double), ("rate_pair_incr", C.c_double),
-                ("reserved", C.c_int32 * 8)]
+                ("i8_min_rows", C.c_int32), ("i8_min_cols", C.c_int32), ("rate_i8_bitops", C.c_double),
+                ("reserved", C.c_int32 * 4)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}

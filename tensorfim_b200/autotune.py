@@ -9,8 +9,11 @@ Parameters (the tfim_tuning table of include/tfim.h):
     (configurations 1, 4 and 5 of tensorfim_b200.synth with their minimum supports, plus
     configuration 4 at 25% of its rows) of the median resident mine time with the learned
     proposal;
-  * rate_b1_bitops, rate_lop3_bitops: bit-ops/s of one 256-node x 512-item counting wave
-    over a random half-dense bitmap of 2^18 transactions, each counter forced;
+  * rate_b1_bitops, rate_lop3_bitops, rate_i8_bitops: bit-ops/s of one 256-node x 512-item
+    counting wave over a random half-dense bitmap of 2^18 transactions, each counter forced
+    (tensorfim_b200.countbench);
+  * i8_min_rows = i8_min_cols: the square wave size from which the tcgen05 kind::i8 counter
+    beats the b1 counter (waves of m x m over 2^20 transactions);
   * rate_pair_incr: pair increments/s of the empty-prefix family counted by pair
     co-occurrence on configuration 4 (sum over reduced rows of len^2/2 over its time).
 Every mine of the sweep is checked against the first one: the table changes speed, never
@@ -63,30 +66,27 @@ def _objective(dbs, reps: int, ref: dict) -> tuple[float, dict]:
 
 
 def _bit_rates(reps: int) -> dict:
-    import torch
-    rng = np.random.Generator(np.random.PCG64(7))
-    n_items, n_bits, b = 512, 1 << 18, 256
-    words = n_bits // 32
-    rows = rng.integers(0, 2 ** 32, size=(n_items, words), dtype=np.uint64).astype(np.uint32)
-    out = {}
-    with Database.from_bitmap(rows, n_bits, n_items) as db:
-        items = torch.arange(b, dtype=torch.int32, device="cuda")
-        offs = torch.arange(b + 1, dtype=torch.int64, device="cuda")
-        counts = torch.zeros((b, n_items), dtype=torch.int32, device="cuda")
-        nfreq = torch.zeros(b, dtype=torch.int32, device="cuda")
-        for counter in ("tensor", "lop3"):
-            db.set_counter(counter)
-            ts = []
-            for k in range(reps + 1):
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record()
-                db.count_wave_device(items.data_ptr(), offs.data_ptr(), b, 1, 1, counts.data_ptr(), nfreq.data_ptr())
-                e1.record()
-                torch.cuda.synchronize()
-                if k:
-                    ts.append(e0.elapsed_time(e1) / 1000.0)
-            out[counter] = b * n_items * n_bits / statistics.median(ts)
-    return {"rate_b1_bitops": out["tensor"], "rate_lop3_bitops": out["lop3"]}
+    from . import countbench
+    r = countbench.run(256, 512, 1 << 18, counters=("tensor", "lop3", "i8"), reps=reps)["counters"]
+    return {"rate_b1_bitops": r["tensor"]["bitops_per_s"], "rate_lop3_bitops": r["lop3"]["bitops_per_s"],
+            "rate_i8_bitops": r["i8"]["bitops_per_s"]}
+
+
+def _i8_crossover(reps: int) -> tuple[int, list]:
+    """Smallest square wave size m (b = d = m nodes x items, 2^20 transactions) from which the
+    tcgen05 kind::i8 counter beats the b1 counter at every larger size measured."""
+    from . import countbench
+    rec = []
+    for m in (32, 64, 96, 128, 192, 256, 384):
+        r = countbench.run(m, m, 1 << 20, counters=("tensor", "i8"), reps=reps)["counters"]
+        rec.append([m, r["tensor"]["seconds"], r["i8"]["seconds"]])
+    best = rec[-1][0] * 2
+    for m, t_b1, t_i8 in reversed(rec):
+        if t_i8 < t_b1:
+            best = m
+        else:
+            break
+    return best, rec
 
 
 def _pair_rate(reps: int) -> float:
@@ -138,6 +138,7 @@ def main() -> None:
         _apply(best)
     rates = _bit_rates(reps)
     rates["rate_pair_incr"] = _pair_rate(reps)
+    i8_min, i8_rec = _i8_crossover(reps)
     for _, db in dbs:
         db.close()
 
@@ -145,7 +146,8 @@ def main() -> None:
              "b1_tiles_per_sm": float(best["b1_tiles_per_sm"]), "b1_min_rows": int(best["b1_min"]),
              "b1_min_cols": int(best["b1_min"]), "proj_auto": int(start["proj_auto"]),
              "rate_b1_bitops": float(rates["rate_b1_bitops"]), "rate_lop3_bitops": float(rates["rate_lop3_bitops"]),
-             "rate_pair_incr": float(rates["rate_pair_incr"])}
+             "rate_pair_incr": float(rates["rate_pair_incr"]), "i8_min_rows": int(i8_min), "i8_min_cols": int(i8_min),
+             "rate_i8_bitops": float(rates["rate_i8_bitops"])}
     import torch
     doc = dict(table)
     doc["measured_on"] = torch.cuda.get_device_name(0)
@@ -154,6 +156,7 @@ def main() -> None:
     doc["sweep_columns"] = ["value", "sum_ms"] + [n for n, _ in dbs]
     for k, rec in sweeps.items():
         doc["sweep:" + k] = rec
+    doc["sweep:i8_crossover"] = {"columns": ["m", "b1_seconds", "i8_seconds"], "rows": i8_rec}
     doc["seconds"] = round(time.time() - t0, 1)
     with open(a.out, "w") as f:
         json.dump(doc, f, indent=1)

@@ -55,7 +55,10 @@ int count_wave_impl(tfim_ctx* c, int32_t b, int32_t min_count, const int32_t* d_
     // host-built job/tile tables (independent of the list contents)
     const int32_t counter = c->counter_pref;
     const tfim_tuning tn = tuning();
-    const bool b1 = counter == TFIM_COUNTER_TENSOR || (counter == TFIM_COUNTER_AUTO && b >= tn.b1_min_rows && d >= tn.b1_min_cols);
+    const bool i8 = counter == TFIM_COUNTER_I8 ||
+                    (counter == TFIM_COUNTER_AUTO && b >= tn.i8_min_rows && d >= tn.i8_min_cols);
+    const bool b1 = !i8 && (counter == TFIM_COUNTER_TENSOR ||
+                            (counter == TFIM_COUNTER_AUTO && b >= tn.b1_min_rows && d >= tn.b1_min_cols));
     std::vector<JobDesc> jobs(1);
     jobs[0].base_slot = -1; jobs[0].base_item = -1;
     jobs[0].n_rows = b; jobs[0].n_cols = d; jobs[0].row_off = 0; jobs[0].col_off = 0; jobs[0].out_off = 0;
@@ -66,7 +69,19 @@ int count_wave_impl(tfim_ctx* c, int32_t b, int32_t min_count, const int32_t* d_
     std::iota(cols.begin(), cols.end(), 0);
     std::vector<TileDesc> tiles;
     const int64_t W = c->W;
-    if (b1) {
+    if (i8) {
+        // 128 x 128 tiles, word slices of 64-word multiples
+        const int64_t base = (int64_t)((b + 127) / 128) * ((d + 127) / 128);
+        const int64_t want = (int64_t)(tn.b1_tiles_per_sm * 148);
+        int64_t ks = std::max<int64_t>(1, (want + base - 1) / base);
+        ks = std::min<int64_t>(ks, W / 64);
+        const int64_t kslice = ((W / 64 + ks - 1) / ks) * 64;
+        for (int64_t w0 = 0; w0 < W; w0 += kslice)
+            for (int32_t r0 = 0; r0 < b; r0 += 128)
+                for (int32_t c0 = 0; c0 < d; c0 += 128)
+                    tiles.push_back(TileDesc{0, r0, std::min(128, b - r0), c0, std::min(d, c0 + 128), (int32_t)w0,
+                                             (int32_t)std::min<int64_t>(W, w0 + kslice), 0});
+    } else if (b1) {
         const int64_t base = (int64_t)((b + kB1Rows - 1) / kB1Rows) * ((d + kB1Cols - 1) / kB1Cols);
         const int64_t want = (int64_t)(tn.b1_tiles_per_sm * 148);
         int64_t ks = std::max<int64_t>(1, (want + base - 1) / base);
@@ -107,7 +122,8 @@ int count_wave_impl(tfim_ctx* c, int32_t b, int32_t min_count, const int32_t* d_
     a.bitmap = c->d_bitmap; a.W = W; a.masks = c->d_masks.as<uint32_t>();
     a.jobs = (const JobDesc*)dp; a.rows = (const RowDesc*)(dp + o_rows); a.cols = (const int32_t*)(dp + o_cols);
     a.tiles = (const TileDesc*)(dp + o_tiles); a.n_tiles = (int32_t)tiles.size(); a.out = d_counts;
-    TFIM_TRY(b1 ? launch_count_b1(a, s) : launch_count_lop3(a, s));
+    c->used_i8 = i8;
+    TFIM_TRY(i8 ? launch_count_i8(a, s) : b1 ? launch_count_b1(a, s) : launch_count_lop3(a, s));
     TFIM_TRY(launch_nfreq(d_counts, b, d, min_count, d_nfreq, s));
     // the host staging buffer may be reused by the next call only after this copy ran
     TFIM_CUDA(cudaStreamSynchronize(s));
@@ -193,7 +209,8 @@ int tfim_dense_freq(const tfim_ctx* c, int32_t* out) {
 
 int tfim_set_counter(tfim_ctx* c, int32_t counter) {
     TFIM_CHECK(c, TFIM_E_INVALID, "null context");
-    TFIM_CHECK(counter >= TFIM_COUNTER_AUTO && counter <= TFIM_COUNTER_TENSOR, TFIM_E_INVALID, "unknown counter %d", counter);
+    TFIM_CHECK((counter >= TFIM_COUNTER_AUTO && counter <= TFIM_COUNTER_TENSOR) || counter == TFIM_COUNTER_I8,
+               TFIM_E_INVALID, "unknown counter %d", counter);
     // (TFIM_COUNTER_PROJ applies to the search's family counts only)
     c->counter_pref = counter;
     return TFIM_OK;
@@ -235,6 +252,7 @@ int tfim_count_wave(tfim_ctx* c, const int32_t* item_lists, const int64_t* list_
     TFIM_CUDA(cudaMemcpyAsync(counts_out, dp + o_counts, (size_t)b * d * 4, cudaMemcpyDeviceToHost, s));
     TFIM_CUDA(cudaMemcpyAsync(nfreq_out, dp + o_nfreq, (size_t)b * 4, cudaMemcpyDeviceToHost, s));
     TFIM_CUDA(cudaStreamSynchronize(s));
+    if (c->used_i8) TFIM_TRY(count_i8_status(true));
     return TFIM_OK;
 }
 

@@ -1348,7 +1348,9 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
         const double nF = n0;
         const bool b1 = o->counter != TFIM_COUNTER_LOP3 &&
                         (o->counter == TFIM_COUNTER_TENSOR || (nF >= tn.b1_min_rows && nF >= tn.b1_min_cols));
-        const double bitmap_s = nF * nF * (double)c->n_bits / 2.0 / (b1 ? tn.rate_b1_bitops : tn.rate_lop3_bitops);
+        const bool i8 = b1 && o->counter != TFIM_COUNTER_TENSOR && nF >= tn.i8_min_rows && nF >= tn.i8_min_cols;
+        const double rate = i8 ? tn.rate_i8_bitops : b1 ? tn.rate_b1_bitops : tn.rate_lop3_bitops;
+        const double bitmap_s = nF * nF * (double)c->n_bits / 2.0 / rate;
         const double pairs_s = c->red_pair_work / 2.0 / tn.rate_pair_incr + nF * nF * 4.0 / kTuneHbmBytes;
         if (o->top_counter == 1) top_mode = 1;
         else if (o->top_counter == 2) top_mode = c->csr_exact ? 2 : 1;
@@ -1356,6 +1358,8 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
     }
     const bool top_b1 = o->counter == TFIM_COUNTER_TENSOR ||
                         (o->counter != TFIM_COUNTER_LOP3 && n0 >= tn.b1_min_rows && n0 >= tn.b1_min_cols);
+    // large families of the empty prefix: the tcgen05 kind::i8 counter, 128 x 128 tiles
+    const bool top_i8 = top_b1 && o->counter != TFIM_COUNTER_TENSOR && n0 >= tn.i8_min_rows && n0 >= tn.i8_min_cols;
 
     const double t_host0 = std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
     double sync_ms = 0, kernel_ms = 0;
@@ -1479,7 +1483,17 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
     {
         std::vector<TileDesc> tl;
         if (top_mode == 1) {
-            if (top_b1) {
+            if (top_i8) {
+                const int64_t g = (n0 + 127) / 128;
+                const int64_t base = g * (g + 1) / 2;   // upper-triangle tiles
+                int64_t ks = std::min<int64_t>(std::max<int64_t>(1, (2LL * sm_count + base - 1) / base), W / 64);
+                const int64_t kslice = ((W / 64 + ks - 1) / ks) * 64;
+                for (int64_t w0 = 0; w0 < W; w0 += kslice)
+                    for (int32_t r0 = 0; r0 < n0; r0 += 128)
+                        for (int32_t c0 = r0; c0 < n0; c0 += 128)
+                            tl.push_back(TileDesc{0, r0, std::min(128, n0 - r0), c0, std::min(n0, c0 + 128), (int32_t)w0,
+                                                  (int32_t)std::min<int64_t>(W, w0 + kslice), 0});
+            } else if (top_b1) {
                 const int64_t base = (int64_t)((n0 + kB1Rows - 1) / kB1Rows) * ((n0 + kB1Cols - 1) / kB1Cols);
                 const int64_t want = (int64_t)(tn.b1_tiles_per_sm * sm_count);
                 int64_t ks = std::min<int64_t>(std::max<int64_t>(1, (want + base - 1) / base), W / 64);
@@ -1513,7 +1527,7 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
         } else {
             a.tiles = top_b1 ? P.tiles_b1 : P.tiles_l3;
             a.n_tiles = (int32_t)tl.size();
-            TFIM_TRY(top_b1 ? launch_count_b1(a, s) : launch_count_lop3(a, s));
+            TFIM_TRY(top_i8 ? launch_count_i8(a, s) : top_b1 ? launch_count_b1(a, s) : launch_count_lop3(a, s));
             bytes_alg += row_bytes * 2 * n0 + 4 * top_out;
         }
         TFIM_CUDA(cudaEventRecord(c->ev1, s));
@@ -1646,6 +1660,7 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
         TFIM_CUDA(cudaMemcpyAsync(c->la_labels.data(), R.log_label.p, (size_t)fin.log_n * 4, cudaMemcpyDeviceToHost, s));
     }
     TFIM_CUDA(cudaStreamSynchronize(s));
+    if (top_i8 && top_mode == 1) TFIM_TRY(count_i8_status(true));
     {
         MfiSet& M = c->mfis;
         const size_t base = M.items.size();

@@ -151,6 +151,10 @@ int launch_count_proj_persistent(const CountArgs* d_args, const int32_t* d_n_job
 // blocks of each persistent kernel resident per SM
 int persistent_occupancy(int* lop3, int* b1, int* proj);
 int configure_count_kernels();
+// tcgen05 kind::i8 counter (count_tc.cu): 128 x 128 tiles; the status reads (and with
+// `reset` clears) the device flag the kernel sets when an mbarrier wait expired.
+int launch_count_i8(const CountArgs& a, cudaStream_t s);
+int count_i8_status(bool reset);
 // The tuning table in force (common.cu): built-in values, or the table loaded / set.
 tfim_tuning tuning();
 int launch_pair_count(const int64_t* red_off, const int32_t* red_items, int64_t n_red, const int32_t* pos,
@@ -230,6 +234,7 @@ struct tfim_ctx {
     tfim::MfiSet mfis;                      // dense ids
     bool mined = false;
     int32_t counter_pref = TFIM_COUNTER_AUTO;   // counter used by tfim_count_wave
+    bool used_i8 = false;                       // the last counting wave ran the tcgen05 i8 counter
     tfim_mine_stats last_stats{};
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     tfim::EngineState* engine = nullptr;

@@ -19,7 +19,7 @@ from ._lib import TfimError, check, lib
 
 ENGINES = {"plain": _lib.ENGINE_PLAIN, "batched": _lib.ENGINE_BATCHED, "resident": _lib.ENGINE_RESIDENT}
 COUNTERS = {"auto": _lib.COUNTER_AUTO, "lop3": _lib.COUNTER_LOP3, "tensor": _lib.COUNTER_TENSOR,
-            "proj": _lib.COUNTER_PROJ}
+            "proj": _lib.COUNTER_PROJ, "i8": _lib.COUNTER_I8}
 
 
 def _ptr(a: np.ndarray) -> C.c_void_p:

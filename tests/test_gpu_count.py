@@ -1,4 +1,4 @@
-"""Counting contract on the GPU: exact integer supports, both counters, against the oracle.
+"""Counting contract on the GPU: exact integer supports, every counter, against the oracle.
 
 Inputs follow the reference microbench's KAT advice (code/microbench/RESULTS.md:39-47):
 sparse random bits (~12.5% density; all-ones data hides layout bugs), b and d not
@@ -42,7 +42,7 @@ SHAPES = [
 ]
 
 
-@pytest.mark.parametrize("counter", ["lop3", "tensor", "auto"])
+@pytest.mark.parametrize("counter", ["lop3", "tensor", "auto", "i8"])
 @pytest.mark.parametrize("shape", SHAPES)
 def test_count_wave_matches_oracle(oracle_mod, shape, counter):
     n_rows, d, n_bits, b, dens = shape
@@ -64,7 +64,7 @@ def test_count_wave_threshold_ties(oracle_mod):
     thr = int(ref_c[1, 5])   # a count exactly at the threshold is frequent
     ref_c, ref_n = oracle_mod.count_wave(rows, lists, 30, thr)
     with tf.Database.from_bitmap(rows, 4096, 30) as db:
-        for counter in ("lop3", "tensor"):
+        for counter in ("lop3", "tensor", "i8"):
             c, n = db.count_wave(lists, thr, counter=counter)
             assert (c == ref_c).all() and (n == ref_n).all()
 

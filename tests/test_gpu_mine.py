@@ -171,3 +171,22 @@ def test_any_tuning_keeps_output(tmp_path, name):
     finally:
         engine.set_tuning(**saved)
 
+
+
+def test_large_top_family_on_every_tensor_path(oracle_mod, tmp_path):
+    """An empty-prefix family of 140 items counted as a bitmap Gram: the automatic choice
+    (tcgen05 kind::i8 tiles from 128 items), b1 tiles and LOP3 tiles all give the oracle's
+    MFI set (every pair frequent, no triple: 9,730 MFIs)."""
+    rng = np.random.Generator(np.random.PCG64(21))
+    x = rng.random((4000, 140)) < 0.6
+    off = np.zeros(x.shape[0] + 1, np.int64)
+    off[1:] = np.cumsum(x.sum(1))
+    items = (np.nonzero(x)[1] + 1).astype(np.int32)
+    p = str(tmp_path / "dense140.txt")
+    synth.write_fimi(p, synth.Database(offsets=off, items=items, n_items=140))
+    exp = oracle_mod.mine_file(p, 0.3)
+    with tf.Database.from_csr(off, items, 0.3) as db:
+        assert db.info["n_survivors"] == 140
+        for counter in ("auto", "tensor", "lop3"):
+            res = db.mine(engine="resident", counter=counter, top="bitmap", lookahead=False)
+            assert res.as_dict() == exp, counter
