@@ -309,13 +309,26 @@ int tfim_mine(tfim_ctx* c, const tfim_mine_opts* opts, tfim_mine_stats* stats) {
     {
         // descending support; ties by descending item lists (deterministic order)
         const MfiSet& M = c->mfis;
-        std::vector<int32_t> idx(M.size());
-        std::iota(idx.begin(), idx.end(), 0);
-        std::sort(idx.begin(), idx.end(), [&](int32_t a, int32_t b) {
+        auto before = [&](int32_t a, int32_t b) {
             if (M.sup[a] != M.sup[b]) return M.sup[a] > M.sup[b];
             return std::lexicographical_compare(M.items.begin() + M.off[b], M.items.begin() + M.off[b + 1],
                                                 M.items.begin() + M.off[a], M.items.begin() + M.off[a + 1]);
-        });
+        };
+        // sort on a packed key (support, first item), then order equal keys fully
+        std::vector<std::pair<uint64_t, int32_t>> keyed(M.size());
+        for (size_t k = 0; k < M.size(); k++) {
+            const uint32_t first = M.off[k + 1] > M.off[k] ? (uint32_t)M.items[M.off[k]] : 0u;
+            keyed[k] = {((uint64_t)(0xFFFFFFFFu - (uint32_t)M.sup[k]) << 32) | (uint64_t)(0xFFFFFFFFu - first), (int32_t)k};
+        }
+        std::sort(keyed.begin(), keyed.end());
+        std::vector<int32_t> idx(M.size());
+        for (size_t k = 0; k < M.size(); k++) idx[k] = keyed[k].second;
+        for (size_t a = 0; a < keyed.size();) {
+            size_t b = a + 1;
+            while (b < keyed.size() && keyed[b].first == keyed[a].first) b++;
+            if (b - a > 1) std::sort(idx.begin() + a, idx.begin() + b, before);
+            a = b;
+        }
         MfiSet S;
         S.items.reserve(M.items.size());
         S.off.reserve(M.size() + 1);

@@ -43,6 +43,12 @@ struct DLook {
     int32_t fam, slot, log, pad;
 };
 
+// A prefix mask to build after an expand: masks[dst] = (slot >= 0 ? masks[slot] : ~0) &
+// (item >= 0 ? B[item] : ~0) & (t >= 0 ? B[t] : ~0) & AND of B[items[off + q]], q < n.
+struct MaskJob {
+    int32_t dst, slot, item, t, off, n, pad0, pad1;
+};
+
 enum { kJobFam = 0, kJobLook = 1 };
 struct DJob {
     int32_t fam, kind, r0, nr, slot, log;
@@ -52,7 +58,7 @@ struct DJob {
 
 struct ResStatus {
     int32_t stack_n, look_n, fam_n, item_n, head_n, mfi_n, mfi_item_n, slot_n, free_n, free_taken, defer_n, log_n;
-    int32_t jobs, rows, tiles_l3, tiles_b1, n_proj, pad0;
+    int32_t jobs, rows, tiles_l3, tiles_b1, n_proj, n_mjobs;   // n_mjobs: masks the last expand asked for
     int64_t out_total;
     int32_t max_cols, max_head, starved, error;
     // grow: the wave the pack built does not fit the pools; nothing was consumed and the
@@ -94,6 +100,7 @@ struct ResPtrs {
     float* log_label;
     // wave
     DJob* djobs;
+    MaskJob* mjobs;
     JobDesc* jobs;
     RowDesc* rows;
     int32_t* row_job;
@@ -230,6 +237,7 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
         s_n_jobs = 0; s_rows_total = 0; s_out_total = 0; s_max_cols = 0; s_max_head = 0; s_done = 0;
         s_stack_after = st->stack_n;
         st->n_proj = 0;
+        st->n_mjobs = 0;
         st->grow = 0;
         st->starved = 0;
         if (st->launch_id != p.launch_id) {
@@ -597,23 +605,32 @@ __device__ __forceinline__ void release_slot(const ResPtrs& p, int32_t s) {
     p.defer[k] = s;
 }
 
-// warp: dst mask row = (slot>=0 ? masks[slot] : ~0) & (item>=0 ? B[item] : ~0) & AND of list
-__device__ void warp_build_mask(const ResPtrs& p, int32_t dst, int32_t slot, int32_t item, int32_t t, const int32_t* extra,
-                                int n_extra, int lane) {
-    const int64_t W4 = p.W >> 2;
-    uint4* d = reinterpret_cast<uint4*>(p.masks + (int64_t)dst * p.W);
-    const uint4* sm = slot >= 0 ? reinterpret_cast<const uint4*>(p.masks + (int64_t)slot * p.W) : nullptr;
-    const uint4* si = item >= 0 ? reinterpret_cast<const uint4*>(p.bitmap + (int64_t)item * p.W) : nullptr;
-    const uint4* st = t >= 0 ? reinterpret_cast<const uint4*>(p.bitmap + (int64_t)t * p.W) : nullptr;
-    for (int64_t w = lane; w < W4; w += 32) {
-        uint4 v = make_uint4(~0u, ~0u, ~0u, ~0u);
-        auto andv = [&](uint4 x) { v.x &= x.x; v.y &= x.y; v.z &= x.z; v.w &= x.w; };
-        if (sm) andv(sm[w]);
-        if (si) andv(__ldg(si + w));
-        if (st) andv(__ldg(st + w));
-        for (int q = 0; q < n_extra; q++) andv(__ldg(reinterpret_cast<const uint4*>(p.bitmap + (int64_t)extra[q] * p.W) + w));
-        d[w] = v;
+// Record a mask for k_build_masks (lane 0 of the calling warp).
+__device__ __forceinline__ void emit_mask(const ResPtrs& p, int32_t dst, int32_t slot, int32_t item, int32_t t, int32_t off,
+                                          int32_t n, int lane) {
+    if (lane == 0) {
+        const int32_t k = atomicAdd(&p.st->n_mjobs, 1);
+        p.mjobs[k] = MaskJob{dst, slot, item, t, off, n, 0, 0};
     }
+}
+
+// Sort an emitted MFI's item list (distinct dense ids) in descending order in place: a rank
+// sort with two items per lane when it holds at most 64 items (longer lists are sorted by the
+// host, which checks every list).
+__device__ void warp_sort_desc(int32_t* a, int n, int lane) {
+    if (n > 64 || n < 2) return;
+    __syncwarp();
+    const int32_t v0 = lane < n ? a[lane] : INT_MIN, v1 = lane + 32 < n ? a[lane + 32] : INT_MIN;
+    int r0 = 0, r1 = 0;
+    for (int j = 0; j < n; j++) {
+        const int32_t x = __shfl_sync(0xffffffffu, j < 32 ? v0 : v1, j & 31);
+        r0 += x > v0;
+        r1 += x > v1;
+    }
+    __syncwarp();
+    if (lane < n) a[r0] = v0;
+    if (lane + 32 < n) a[r1] = v1;
+    __syncwarp();
 }
 
 __device__ void warp_emit_mfi(const ResPtrs& p, const int32_t* head, int head_len, int32_t t, const int32_t* extra_cols,
@@ -636,6 +653,7 @@ __device__ void warp_emit_mfi(const ResPtrs& p, const int32_t* head, int head_le
     for (int q = lane; q < head_len; q += 32) p.mfi_items[off + q] = head[q];
     if (lane == 0) p.mfi_items[off + head_len] = t;
     for (int q = lane; q < n_extra; q += 32) p.mfi_items[off + head_len + 1 + q] = F[extra_cols[q]];
+    warp_sort_desc(p.mfi_items + off, len, lane);
     if (lane == 0) {
         p.mfi_off[k] = off;
         p.mfi_len[k] = len;
@@ -725,6 +743,7 @@ __device__ void expand_row(const ResPtrs& p, int64_t g, int lane) {
                     off = __shfl_sync(0xffffffffu, off, 0);
                     for (int q = lane; q < f.head_len; q += 32) p.mfi_items[off + q] = head[q];
                     for (int q = lane; q < f.nT; q += 32) p.mfi_items[off + f.head_len + q] = F[q];
+                    warp_sort_desc(p.mfi_items + off, len, lane);
                     if (lane == 0) {
                         p.mfi_off[k] = off;
                         p.mfi_len[k] = len;
@@ -900,7 +919,7 @@ __device__ void expand_row(const ResPtrs& p, int64_t g, int lane) {
     } else {
         if (lane == 0) cslot = pop_slot(p);
         cslot = __shfl_sync(0xffffffffu, cslot, 0);
-        warp_build_mask(p, cslot, f.slot, f.item, t, nullptr, 0, lane);
+        emit_mask(p, cslot, f.slot, f.item, t, 0, 0, lane);
     }
     // lookahead decision
     bool issue = false;
@@ -1005,9 +1024,8 @@ __device__ void expand_row(const ResPtrs& p, int64_t g, int lane) {
         int32_t ls = 0;
         if (lane == 0) ls = pop_slot(p);
         ls = __shfl_sync(0xffffffffu, ls, 0);
-        // mask of head + tail: child base & the tail rows
-        if (cslot >= 0) warp_build_mask(p, ls, cslot, -1, -1, Fc, n_tail, lane);
-        else warp_build_mask(p, ls, -1, citem, -1, Fc, n_tail, lane);
+        // mask of head + tail: the child's base (the parent's sources and t) & the tail rows
+        emit_mask(p, ls, f.slot, f.item, t, foff, n_tail, lane);
         if (lane == 0) {
             const int32_t q = atomicAdd(&st->look_n, 1);
             p.looks[q] = DLook{fid, ls, log_idx, 0};
@@ -1026,6 +1044,35 @@ __global__ void __launch_bounds__(256) k_res_expand(ResPtrs p) {
     if (g >= p.st->rows) return;
     expand_row(p, g, threadIdx.x & 31);
 }
+
+// The masks the expand asked for, with the whole grid: units of 1,024 128-bit words of one
+// mask, strided over the blocks (one warp building a 1,000,000-bit mask alone would take a
+// chain of ~250 dependent load rounds).
+__device__ __forceinline__ void build_masks(const ResPtrs& p) {
+    const int32_t n = p.st->n_mjobs;
+    const int64_t W4 = p.W >> 2;
+    const int64_t chunks = (W4 + 1023) / 1024;
+    const uint4 ones = make_uint4(~0u, ~0u, ~0u, ~0u);
+    for (int64_t u = blockIdx.x; u < (int64_t)n * chunks; u += gridDim.x) {
+        const MaskJob mj = p.mjobs[u / chunks];
+        const int64_t c0 = (u % chunks) * 1024, c1 = lmin(W4, c0 + 1024);
+        uint4* d = reinterpret_cast<uint4*>(p.masks + (int64_t)mj.dst * p.W);
+        const uint4* sm = mj.slot >= 0 ? reinterpret_cast<const uint4*>(p.masks + (int64_t)mj.slot * p.W) : nullptr;
+        const uint4* si = mj.item >= 0 ? reinterpret_cast<const uint4*>(p.bitmap + (int64_t)mj.item * p.W) : nullptr;
+        const uint4* st = mj.t >= 0 ? reinterpret_cast<const uint4*>(p.bitmap + (int64_t)mj.t * p.W) : nullptr;
+        for (int64_t w = c0 + threadIdx.x; w < c1; w += blockDim.x) {
+            uint4 v = ones;
+            auto andv = [&](uint4 x) { v.x &= x.x; v.y &= x.y; v.z &= x.z; v.w &= x.w; };
+            if (sm) andv(sm[w]);
+            if (si) andv(__ldg(si + w));
+            if (st) andv(__ldg(st + w));
+            for (int q = 0; q < mj.n; q++)
+                andv(__ldg(reinterpret_cast<const uint4*>(p.bitmap + (int64_t)p.items[mj.off + q] * p.W) + w));
+            d[w] = v;
+        }
+    }
+}
+__global__ void __launch_bounds__(256) k_build_masks(ResPtrs p) { build_masks(p); }
 
 // The expand's first pass for the family of the empty prefix (an n x n count block whose
 // rows are its tail, nT = nF = n): one block per row streams the row with four loads in
@@ -1106,6 +1153,11 @@ __global__ void __launch_bounds__(256) k_res_expand_g(const ResArgs* __restrict_
     for (int64_t g = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; g < rows; g += warps) expand_row(p, g, lane);
 }
 
+__global__ void __launch_bounds__(256) k_build_masks_g(const ResArgs* __restrict__ args) {
+    const ResPtrs p = args->p;
+    build_masks(p);
+}
+
 __global__ void k_res_control(const ResArgs* __restrict__ args, cudaGraphConditionalHandle h) {
     if (threadIdx.x != 0) return;
     ResStatus* st = args->p.st;
@@ -1181,6 +1233,7 @@ int build_wave_graph(WaveGraph& G, const ResArgs* d_args, ResStatus* d_status, b
             (rc = launch_count_proj_persistent(&d_args->a3, &d_status->n_proj, sm * std::max(1, occp), red_off, red_items, s)))
             break;
         k_res_expand_g<<<sm * std::max(1, occe), 256, 0, s>>>(d_args);
+        k_build_masks_g<<<sm * 8, 256, 0, s>>>(d_args);
         k_res_control<<<1, 32, 0, s>>>(d_args, h);
     } while (0);
     cudaGraph_t captured = nullptr;
@@ -1200,21 +1253,23 @@ int build_wave_graph(WaveGraph& G, const ResArgs* d_args, ResStatus* d_status, b
 struct ResidentState {
     Pool fams, items, heads, stack, looks, free_slots, defer, mfi_off, mfi_len, mfi_sup, mfi_items, log_feat, log_label;
     Pool djobs, jobs, rows, row_job, row_local, tiles_l3, tiles_b1, counts, status, is_root, dense_freq, top_pos, top_diag,
-        proj_list, args, top_sum;
-    HostBuf h_status, h_args;
+        proj_list, args, top_sum, mjobs;
+    HostBuf h_status, h_args, h_res, h_setup;
     WaveGraph graph;
     int32_t launch_id = 0;
     void release(cudaStream_t s) {
         graph.release();
         for (Pool* b : {&fams, &items, &heads, &stack, &looks, &free_slots, &defer, &mfi_off, &mfi_len, &mfi_sup, &mfi_items,
                         &log_feat, &log_label, &djobs, &jobs, &rows, &row_job, &row_local, &tiles_l3, &tiles_b1, &counts,
-                        &status, &is_root, &dense_freq, &top_pos, &top_diag, &proj_list, &args, &top_sum}) {
+                        &status, &is_root, &dense_freq, &top_pos, &top_diag, &proj_list, &args, &top_sum, &mjobs}) {
             dev_free(b->p, s);
             b->p = nullptr;
             b->bytes = 0;
         }
         h_status.release();
         h_args.release();
+        h_res.release();
+        h_setup.release();
     }
 };
 
@@ -1292,6 +1347,7 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
     TFIM_TRY(grow(R.row_job, cap_rows * 4, s));
     TFIM_TRY(grow(R.row_local, cap_rows * 4, s));
     TFIM_TRY(grow(R.proj_list, cap_rows * 4, s));
+    TFIM_TRY(grow(R.mjobs, (2 * cap_rows + 2) * sizeof(MaskJob), s));   // at most two masks per expanded row
     TFIM_TRY(grow(R.tiles_l3, cap_tiles * sizeof(TileDesc), s));
     TFIM_TRY(grow(R.tiles_b1, cap_tiles * sizeof(TileDesc), s));
     TFIM_TRY(grow(R.counts, cap_out * 4, s));
@@ -1299,17 +1355,15 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
     TFIM_TRY(grow(R.dense_freq, (size_t)std::max<int32_t>(c->info.n_dense, 1) * 4, s));
     TFIM_TRY(grow(R.top_pos, (size_t)std::max<int32_t>(c->info.n_dense, 1) * 4, s));
     TFIM_TRY(grow(R.top_diag, (size_t)n0 * 4, s));
-    TFIM_CUDA(cudaMemcpyAsync(R.is_root.p, is_root.data(), is_root.size(), cudaMemcpyHostToDevice, s));
-    TFIM_CUDA(cudaMemcpyAsync(R.dense_freq.p, c->dense_freq.data(), c->dense_freq.size() * 4, cudaMemcpyHostToDevice, s));
     // mask slots (grown on demand)
     int64_t slot_cap = c->d_masks.bytes / ((size_t)W * 4);
 
-    // the top family record and its single job
+    // the search's initial state, staged in pinned memory and copied asynchronously:
+    // root flags, F1 counts, the top family record, its F list and its single job, rows,
+    // F positions and row supports, the status record
     DFam top;
     top.slot = -1; top.item = -1; top.head_off = 0; top.head_len = 0; top.F_off = 0; top.nF = n0; top.nT = n0;
     top.sup = 0; top.next_row = n0; top.rows_done = 0; top.state = 0; top.top = 1;
-    TFIM_CUDA(cudaMemcpyAsync(R.fams.p, &top, sizeof top, cudaMemcpyHostToDevice, s));
-    TFIM_CUDA(cudaMemcpyAsync(R.items.p, F0.data(), (size_t)n0 * 4, cudaMemcpyHostToDevice, s));
     ResStatus hs;
     memset(&hs, 0, sizeof hs);
     hs.fam_n = 1;
@@ -1321,24 +1375,47 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
     hs.nodes = n0;
     hs.supports = (unsigned long long)top_out;
     {
-        std::vector<DJob> dj(1);
-        dj[0] = DJob{0, kJobFam, 0, n0, -1, -1, 0, 0, 0, 1};
-        std::vector<JobDesc> jd(1);
-        jd[0] = JobDesc{-1, -1, n0, n0, 0, 0, 0, -1, 0};
-        std::vector<RowDesc> rows(n0);
-        std::vector<int32_t> rj(n0, 0), rl(n0);
-        for (int32_t k = 0; k < n0; k++) { rows[k] = RowDesc{-1, F0[k]}; rl[k] = k; }
-        TFIM_CUDA(cudaMemcpyAsync(R.djobs.p, dj.data(), sizeof(DJob), cudaMemcpyHostToDevice, s));
-        TFIM_CUDA(cudaMemcpyAsync(R.jobs.p, jd.data(), sizeof(JobDesc), cudaMemcpyHostToDevice, s));
-        TFIM_CUDA(cudaMemcpyAsync(R.rows.p, rows.data(), (size_t)n0 * sizeof(RowDesc), cudaMemcpyHostToDevice, s));
-        TFIM_CUDA(cudaMemcpyAsync(R.row_job.p, rj.data(), (size_t)n0 * 4, cudaMemcpyHostToDevice, s));
-        TFIM_CUDA(cudaMemcpyAsync(R.row_local.p, rl.data(), (size_t)n0 * 4, cudaMemcpyHostToDevice, s));
-        std::vector<int32_t> pos((size_t)std::max<int32_t>(c->info.n_dense, 1), -1), diag(n0);
-        for (int32_t k = 0; k < n0; k++) { pos[F0[k]] = k; diag[k] = c->bit_support[F0[k]]; }
-        TFIM_CUDA(cudaMemcpyAsync(R.top_pos.p, pos.data(), pos.size() * 4, cudaMemcpyHostToDevice, s));
-        TFIM_CUDA(cudaMemcpyAsync(R.top_diag.p, diag.data(), (size_t)n0 * 4, cudaMemcpyHostToDevice, s));
+        const size_t nd = (size_t)std::max<int32_t>(c->info.n_dense, 1);
+        struct Part { void* dst; size_t off, bytes; };
+        std::vector<Part> parts;
+        size_t total = 0;
+        auto part = [&](void* dst, size_t bytes) {
+            parts.push_back(Part{dst, total, bytes});
+            total += (bytes + 15) & ~size_t(15);
+            return parts.size() - 1;
+        };
+        const size_t p_root = part(R.is_root.p, is_root.size()), p_freq = part(R.dense_freq.p, c->dense_freq.size() * 4),
+                     p_fam = part(R.fams.p, sizeof(DFam)), p_F = part(R.items.p, (size_t)n0 * 4),
+                     p_dj = part(R.djobs.p, sizeof(DJob)), p_jd = part(R.jobs.p, sizeof(JobDesc)),
+                     p_rows = part(R.rows.p, (size_t)n0 * sizeof(RowDesc)), p_rj = part(R.row_job.p, (size_t)n0 * 4),
+                     p_rl = part(R.row_local.p, (size_t)n0 * 4), p_pos = part(R.top_pos.p, nd * 4),
+                     p_diag = part(R.top_diag.p, (size_t)n0 * 4), p_st = part(R.status.p, sizeof(ResStatus));
+        TFIM_TRY(R.h_setup.reserve(total));
+        unsigned char* h = R.h_setup.as<unsigned char>();
+        auto at = [&](size_t k) { return (void*)(h + parts[k].off); };
+        memcpy(at(p_root), is_root.data(), is_root.size());
+        memcpy(at(p_freq), c->dense_freq.data(), c->dense_freq.size() * 4);
+        memcpy(at(p_fam), &top, sizeof top);
+        memcpy(at(p_F), F0.data(), (size_t)n0 * 4);
+        *(DJob*)at(p_dj) = DJob{0, kJobFam, 0, n0, -1, -1, 0, 0, 0, 1};
+        *(JobDesc*)at(p_jd) = JobDesc{-1, -1, n0, n0, 0, 0, 0, -1, 0};
+        RowDesc* rows = (RowDesc*)at(p_rows);
+        int32_t* rj = (int32_t*)at(p_rj);
+        int32_t* rl = (int32_t*)at(p_rl);
+        int32_t* pos = (int32_t*)at(p_pos);
+        int32_t* diag = (int32_t*)at(p_diag);
+        std::fill(pos, pos + nd, -1);
+        for (int32_t k = 0; k < n0; k++) {
+            rows[k] = RowDesc{-1, F0[k]};
+            rj[k] = 0;
+            rl[k] = k;
+            pos[F0[k]] = k;
+            diag[k] = c->bit_support[F0[k]];
+        }
+        memcpy(at(p_st), &hs, sizeof hs);
+        for (const Part& q : parts)
+            if (q.bytes) TFIM_CUDA(cudaMemcpyAsync(q.dst, h + q.off, q.bytes, cudaMemcpyHostToDevice, s));
     }
-    TFIM_CUDA(cudaMemcpyAsync(R.status.p, &hs, sizeof hs, cudaMemcpyHostToDevice, s));
     TFIM_TRY(R.h_status.reserve(sizeof(ResStatus)));
     ResStatus* hst = R.h_status.as<ResStatus>();
 
@@ -1374,6 +1451,7 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
         P.mfi_sup = (int32_t*)R.mfi_sup.p; P.mfi_items = (int32_t*)R.mfi_items.p;
         P.log_feat = (float*)R.log_feat.p; P.log_label = (float*)R.log_label.p;
         P.djobs = (DJob*)R.djobs.p; P.jobs = (JobDesc*)R.jobs.p; P.rows = (RowDesc*)R.rows.p;
+        P.mjobs = (MaskJob*)R.mjobs.p;
         P.row_job = (int32_t*)R.row_job.p; P.row_local = (int32_t*)R.row_local.p;
         P.tiles_l3 = (TileDesc*)R.tiles_l3.p; P.tiles_b1 = (TileDesc*)R.tiles_b1.p; P.counts = (int32_t*)R.counts.p;
         P.bitmap = c->d_bitmap; P.masks = c->d_masks.as<uint32_t>(); P.dense_freq = (const int32_t*)R.dense_freq.p;
@@ -1542,6 +1620,9 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
         Ptop.row_sum = (const RowSum*)R.top_sum.p;
         k_res_expand<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(Ptop);
         TFIM_CUDA(cudaGetLastError());
+        k_build_masks<<<sm_count * 8, 256, 0, s>>>(P);
+        TFIM_CUDA(cudaGetLastError());
+        launches++;
         launches++;
         waves++;
         float ms = 0;
@@ -1589,8 +1670,8 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
             if (hst->jobs == 0) break;   // the stack and the lookahead queue are empty
             TFIM_CHECK(slices < (1LL << 40), TFIM_E_STATE, "resident search did not finish");
         }
-        // per wave: pack, zero, lop3, b1, [proj], expand, control
-        launches += (int64_t)hst->waves * (6 + (with_proj ? 1 : 0));
+        // per wave: pack, zero, lop3, b1, [proj], expand, masks, control
+        launches += (int64_t)hst->waves * (7 + (with_proj ? 1 : 0));
         count_launches += (int64_t)hst->waves * (2 + (with_proj ? 1 : 0));
         kernel_ms += (double)hst->count_ns * 1e-6;
     }
@@ -1636,6 +1717,9 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
         const int64_t threads = (int64_t)hst->rows * 32;
         k_res_expand<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(P);
         TFIM_CUDA(cudaGetLastError());
+        k_build_masks<<<sm_count * 8, 256, 0, s>>>(P);
+        TFIM_CUDA(cudaGetLastError());
+        launches++;
         launches++;
         host_waves++;
         float ms = 0;
@@ -1646,12 +1730,18 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
     waves += use_graph ? (int64_t)hst->waves : host_waves;
     // results
     const ResStatus fin = *hst;
-    std::vector<int32_t> moff(fin.mfi_n), mlen(fin.mfi_n), msup(fin.mfi_n), mitems(fin.mfi_item_n);
-    if (fin.mfi_n) {
-        TFIM_CUDA(cudaMemcpyAsync(moff.data(), R.mfi_off.p, (size_t)fin.mfi_n * 4, cudaMemcpyDeviceToHost, s));
-        TFIM_CUDA(cudaMemcpyAsync(mlen.data(), R.mfi_len.p, (size_t)fin.mfi_n * 4, cudaMemcpyDeviceToHost, s));
-        TFIM_CUDA(cudaMemcpyAsync(msup.data(), R.mfi_sup.p, (size_t)fin.mfi_n * 4, cudaMemcpyDeviceToHost, s));
-        TFIM_CUDA(cudaMemcpyAsync(mitems.data(), R.mfi_items.p, (size_t)fin.mfi_item_n * 4, cudaMemcpyDeviceToHost, s));
+    // the MFI pool through one pinned staging buffer: offsets, lengths, supports, items
+    const size_t nm = (size_t)fin.mfi_n, ni = (size_t)fin.mfi_item_n;
+    TFIM_TRY(R.h_res.reserve((3 * nm + ni + 1) * 4));
+    int32_t* moff = R.h_res.as<int32_t>();
+    int32_t* mlen = moff + nm;
+    int32_t* msup = mlen + nm;
+    int32_t* mitems = msup + nm;
+    if (nm) {
+        TFIM_CUDA(cudaMemcpyAsync(moff, R.mfi_off.p, nm * 4, cudaMemcpyDeviceToHost, s));
+        TFIM_CUDA(cudaMemcpyAsync(mlen, R.mfi_len.p, nm * 4, cudaMemcpyDeviceToHost, s));
+        TFIM_CUDA(cudaMemcpyAsync(msup, R.mfi_sup.p, nm * 4, cudaMemcpyDeviceToHost, s));
+        TFIM_CUDA(cudaMemcpyAsync(mitems, R.mfi_items.p, ni * 4, cudaMemcpyDeviceToHost, s));
     }
     if (o->log_lookahead && fin.log_n) {
         c->la_feats.resize((size_t)fin.log_n * 32);
@@ -1670,8 +1760,9 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
         size_t o = base;
         for (int32_t k = 0; k < fin.mfi_n; k++) {
             int32_t* dst = M.items.data() + o;
-            std::copy(mitems.begin() + moff[k], mitems.begin() + moff[k] + mlen[k], dst);
-            std::sort(dst, dst + mlen[k], std::greater<int32_t>());
+            std::copy(mitems + moff[k], mitems + moff[k] + mlen[k], dst);
+            if (!std::is_sorted(dst, dst + mlen[k], std::greater<int32_t>()))   // lists over 64 items
+                std::sort(dst, dst + mlen[k], std::greater<int32_t>());
             o += (size_t)mlen[k];
             M.off.push_back((int64_t)o);
             M.sup.push_back(msup[k]);
