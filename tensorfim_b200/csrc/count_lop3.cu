@@ -42,7 +42,8 @@ struct Lop3Shared {
 
 __device__ __forceinline__ bool nonzero4(uint4 v) { return (v.x | v.y | v.z | v.w) != 0u; }
 
-__device__ void lop3_tile(const CountArgs& a, const TileDesc t, Lop3Shared& sh) {
+template <bool WIDE>
+__device__ void lop3_tile_impl(const CountArgs& a, const TileDesc t, Lop3Shared& sh) {
     const JobDesc j = a.jobs[t.job];
     const int64_t W = a.W;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -57,15 +58,16 @@ __device__ void lop3_tile(const CountArgs& a, const TileDesc t, Lop3Shared& sh) 
     const uint4* base_m = j.base_slot >= 0 ? reinterpret_cast<const uint4*>(a.masks + (int64_t)j.base_slot * W) : nullptr;
     const uint4* base_i = j.base_item >= 0 ? reinterpret_cast<const uint4*>(a.bitmap + (int64_t)j.base_item * W) : nullptr;
     // flush layout: G staged positions per pass, lane -> (position offset, column(s))
-    const bool wide = ncols > 32;
+    constexpr bool wide = WIDE;
+    constexpr int NC = WIDE ? 2 : 1;   // columns per lane
     const int G = wide ? 1 : 32 / ncols;
     const int koff = wide ? 0 : lane / ncols;
     const bool active = koff < G;
     const int cl[2] = {wide ? lane : lane % ncols, wide ? lane + 32 : -1};
-    const uint4* cp[2];
-    int ck[2];   // 0: column row, 1: all ones, 2: none
+    const uint4* cp[NC];
+    int ck[NC];   // 0: column row, 1: all ones, 2: none
 #pragma unroll
-    for (int ci = 0; ci < 2; ci++) {
+    for (int ci = 0; ci < NC; ci++) {
         const int c = t.c0 + cl[ci];
         ck[ci] = 2;
         cp[ci] = nullptr;
@@ -77,9 +79,9 @@ __device__ void lop3_tile(const CountArgs& a, const TileDesc t, Lop3Shared& sh) 
             }
         }
     }
-    uint32_t acc[2][kLop3Rows];
+    uint32_t acc[NC][kLop3Rows];
 #pragma unroll
-    for (int ci = 0; ci < 2; ci++)
+    for (int ci = 0; ci < NC; ci++)
 #pragma unroll
         for (int r = 0; r < kLop3Rows; r++) acc[ci][r] = 0;
     __syncthreads();   // rsrc, acc
@@ -94,17 +96,17 @@ __device__ void lop3_tile(const CountArgs& a, const TileDesc t, Lop3Shared& sh) 
             const int k = k0 + koff;
             if (!active || k >= ns) continue;
             const int p = wpos[k];
-            uint4 v[2];
+            uint4 v[NC];
 #pragma unroll
-            for (int ci = 0; ci < 2; ci++)
+            for (int ci = 0; ci < NC; ci++)
                 v[ci] = ck[ci] == 0 ? __ldg(cp[ci] + p) : ck[ci] == 1 ? make_uint4(~0u, ~0u, ~0u, ~0u) : make_uint4(0, 0, 0, 0);
             const uint4* st = wst + k * nr;
 #pragma unroll
             for (int r = 0; r < kLop3Rows; r++) {
                 if (r >= nr) break;
                 const uint4 m = st[r];
-                acc[0][r] += popc4(and4(m, v[0]));
-                if (wide) acc[1][r] += popc4(and4(m, v[1]));
+#pragma unroll
+                for (int ci = 0; ci < NC; ci++) acc[ci][r] += popc4(and4(m, v[ci]));
             }
         }
         __syncwarp();
@@ -162,7 +164,7 @@ __device__ void lop3_tile(const CountArgs& a, const TileDesc t, Lop3Shared& sh) 
     if (ns > 0) flush();
     // partial sums of the warps meet in shared memory; one global atomic per output
 #pragma unroll
-    for (int ci = 0; ci < 2; ci++)
+    for (int ci = 0; ci < NC; ci++)
 #pragma unroll
         for (int r = 0; r < kLop3Rows; r++)
             if (r < nr && ck[ci] != 2 && acc[ci][r]) atomicAdd(&sh.acc[r * 64 + cl[ci]], (int32_t)acc[ci][r]);
@@ -173,6 +175,12 @@ __device__ void lop3_tile(const CountArgs& a, const TileDesc t, Lop3Shared& sh) 
         if (v) atomicAdd(a.out + j.out_off + (int64_t)(t.r0 + r) * j.n_cols + t.c0 + c, v);
     }
     __syncthreads();   // shared state is reused by the block's next tile
+}
+
+// Tiles of more than 32 columns give each lane two columns.
+__device__ __forceinline__ void lop3_tile(const CountArgs& a, const TileDesc t, Lop3Shared& sh) {
+    if (t.c1 - t.c0 > 32) lop3_tile_impl<true>(a, t, sh);
+    else lop3_tile_impl<false>(a, t, sh);
 }
 
 __global__ void __launch_bounds__(256, 4) k_count_lop3(CountArgs a) {

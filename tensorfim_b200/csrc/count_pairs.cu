@@ -33,13 +33,25 @@ __global__ void k_pair_count(const int64_t* __restrict__ red_off, const int32_t*
     }
 }
 
-// M[j][i] = M[i][j] for i < j; M[i][i] = diag[i].
-__global__ void k_mirror(int32_t* __restrict__ M, int32_t nF, const int32_t* __restrict__ diag) {
-    const int64_t n = (int64_t)nF * nF;
-    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
-        const int32_t i = (int32_t)(k / nF), j = (int32_t)(k % nF);
-        if (j < i) M[k] = M[(int64_t)j * nF + i];
-        else if (j == i && diag) M[k] = diag[i];
+// M[j][i] = M[i][j] for i < j; M[i][i] = diag[i] (when given).  One 32 x 32 tile per block,
+// transposed through shared memory so that both the upper-triangle reads and the
+// lower-triangle writes are coalesced.  Blocks read only entries above the diagonal and
+// write only entries on or below it, so no block reads what another writes.
+__global__ void __launch_bounds__(256) k_mirror(int32_t* __restrict__ M, int32_t nF, const int32_t* __restrict__ diag) {
+    __shared__ int32_t tile[32][33];
+    const int32_t bi = blockIdx.x, bj = blockIdx.y;   // destination rows bi, columns bj
+    if (bj > bi) return;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;   // 32 x 8 threads
+    for (int k = ty; k < 32; k += 8) {
+        const int64_t r = (int64_t)bj * 32 + k, c = (int64_t)bi * 32 + tx;   // source: upper triangle
+        tile[k][tx] = r < nF && c < nF && r < c ? M[r * nF + c] : 0;
+    }
+    __syncthreads();
+    for (int k = ty; k < 32; k += 8) {
+        const int64_t r = (int64_t)bi * 32 + k, c = (int64_t)bj * 32 + tx;
+        if (r >= nF || c >= nF) continue;
+        if (c < r) M[r * nF + c] = tile[tx][k];
+        else if (c == r && diag) M[r * nF + c] = diag[r];
     }
 }
 
@@ -57,10 +69,9 @@ int launch_pair_count(const int64_t* red_off, const int32_t* red_items, int64_t 
 
 int launch_mirror(int32_t* M, int32_t nF, const int32_t* diag, cudaStream_t s) {
     if (nF <= 0) return TFIM_OK;
-    const int64_t n = (int64_t)nF * nF;
-    int64_t blocks = (n + 255) / 256;
-    if (blocks > 148 * 32) blocks = 148 * 32;
-    k_mirror<<<(unsigned)blocks, 256, 0, s>>>(M, nF, diag);
+    const unsigned nb = (unsigned)((nF + 31) / 32);
+    TFIM_CHECK(nb <= 65535, TFIM_E_INVALID, "family of %d items exceeds the mirror grid", nF);
+    k_mirror<<<dim3(nb, nb), 256, 0, s>>>(M, nF, diag);
     TFIM_CUDA(cudaGetLastError());
     return TFIM_OK;
 }
