@@ -90,6 +90,30 @@ __global__ void k_hist(const int32_t* __restrict__ items, int64_t nnz, int32_t* 
         atomicAdd(&freq[items[j]], 1);
 }
 
+// The same histogram when the id space fits in shared memory: every block counts a strided
+// share of the items in a private shared histogram (no global atomics; the skewed ids of a
+// long-tailed database collide only within a block) and writes it to partial[block]; the
+// column sums are taken by k_hist_sum.
+constexpr int kHistSmemBins = 48 * 1024;
+__global__ void __launch_bounds__(1024) k_hist_smem(const int32_t* __restrict__ items, int64_t nnz, int32_t bins,
+                                                    int32_t* __restrict__ partial) {
+    extern __shared__ int32_t h[];
+    for (int i = threadIdx.x; i < bins; i += blockDim.x) h[i] = 0;
+    __syncthreads();
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < nnz; j += (int64_t)gridDim.x * blockDim.x)
+        atomicAdd(&h[__ldg(items + j)], 1);
+    __syncthreads();
+    int32_t* out = partial + (int64_t)blockIdx.x * bins;
+    for (int i = threadIdx.x; i < bins; i += blockDim.x) out[i] = h[i];
+}
+__global__ void k_hist_sum(const int32_t* __restrict__ partial, int32_t parts, int32_t bins, int32_t* __restrict__ freq) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= bins) return;
+    int32_t v = 0;
+    for (int b = 0; b < parts; b++) v += partial[(int64_t)b * bins + i];
+    freq[i] = v;
+}
+
 // Per row: the reduced length (occurrences of ids that survive the threshold, id 0
 // included when frequent); 0 marks a row that reduction removes.
 __global__ void k_reduced_rows(const int64_t* __restrict__ off, const int32_t* __restrict__ items, int64_t n_rows,
@@ -254,8 +278,25 @@ int ingest_csr(tfim_ctx* c, const int64_t* h_off, const int32_t* h_items, int64_
 
     // F1 histogram over ids 0..id_max (kernel_bitmap.cu:269-275)
     if ((rc = d_freq.reserve((size_t)(id_max + 1) * 4))) return done(rc);
-    cudaMemsetAsync(d_freq.p, 0, (size_t)(id_max + 1) * 4, s);
-    if (nnz > 0) k_hist<<<grid_for(nnz), 256, 0, s>>>(d_items.as<int32_t>(), nnz, d_freq.as<int32_t>());
+    {
+        const int32_t bins = (int32_t)(id_max + 1);
+        if (nnz > 0 && bins <= kHistSmemBins) {
+            const int32_t parts = (int32_t)std::min<int64_t>(148, (nnz + 65535) / 65536);
+            if ((rc = d_tmp.reserve((size_t)parts * bins * 4))) return done(rc);
+            static bool configured[64] = {};
+            int dev = 0;
+            cudaGetDevice(&dev);
+            if (dev >= 0 && dev < 64 && !configured[dev]) {
+                cudaFuncSetAttribute(k_hist_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, kHistSmemBins * 4);
+                configured[dev] = true;
+            }
+            k_hist_smem<<<parts, 1024, (size_t)bins * 4, s>>>(d_items.as<int32_t>(), nnz, bins, d_tmp.as<int32_t>());
+            k_hist_sum<<<(bins + 255) / 256, 256, 0, s>>>(d_tmp.as<int32_t>(), parts, bins, d_freq.as<int32_t>());
+        } else {
+            cudaMemsetAsync(d_freq.p, 0, (size_t)bins * 4, s);
+            if (nnz > 0) k_hist<<<grid_for(nnz), 256, 0, s>>>(d_items.as<int32_t>(), nnz, d_freq.as<int32_t>());
+        }
+    }
     freq.assign((size_t)id_max + 1, 0);
     cudaMemcpyAsync(freq.data(), d_freq.p, (size_t)(id_max + 1) * 4, cudaMemcpyDeviceToHost, s);
     if (cudaStreamSynchronize(s) != cudaSuccess) { set_error("F1 histogram failed: %s", cudaGetErrorString(cudaGetLastError())); return done(TFIM_E_CUDA); }
