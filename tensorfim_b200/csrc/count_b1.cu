@@ -211,12 +211,21 @@ __global__ void __launch_bounds__(256) k_count_b1(CountArgs a) {
     b1_tile(a, a.tiles[blockIdx.x], smem, sh);
 }
 
-__global__ void __launch_bounds__(256) k_count_b1_persistent(const CountArgs* __restrict__ args, const int32_t* n_tiles) {
+__global__ void __launch_bounds__(256) k_count_b1_persistent(const CountArgs* __restrict__ args, const int32_t* n_tiles,
+                                                             int32_t* next) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ B1Shared sh;
+    __shared__ int32_t s_t;
     const CountArgs a = *args;
     const int32_t n = *n_tiles;
-    for (int32_t t = blockIdx.x; t < n; t += gridDim.x) b1_tile(a, a.tiles[t], smem, sh);
+    while (true) {
+        if (threadIdx.x == 0) s_t = atomicAdd(next, 1);
+        __syncthreads();
+        const int32_t t = s_t;
+        __syncthreads();
+        if (t >= n) break;
+        b1_tile(a, a.tiles[t], smem, sh);
+    }
 }
 
 }  // namespace
@@ -250,10 +259,11 @@ int occupancy_b1(int* blocks) {
     return TFIM_OK;
 }
 
-int launch_count_b1_persistent(const CountArgs* d_args, const int32_t* d_n_tiles, int32_t grid, cudaStream_t s) {
+int launch_count_b1_persistent(const CountArgs* d_args, const int32_t* d_n_tiles, int32_t* d_next, int32_t grid,
+                               cudaStream_t s) {
     TFIM_TRY(configure_count_kernels());
     const size_t smem = (size_t)kStages * kStageBytes;
-    k_count_b1_persistent<<<grid, 256, smem, s>>>(d_args, d_n_tiles);
+    k_count_b1_persistent<<<grid, 256, smem, s>>>(d_args, d_n_tiles, d_next);
     TFIM_CUDA(cudaGetLastError());
     return TFIM_OK;
 }

@@ -188,13 +188,23 @@ __global__ void __launch_bounds__(256, 4) k_count_lop3(CountArgs a) {
     lop3_tile(a, a.tiles[blockIdx.x], sh);
 }
 
-// Persistent form: arguments and tile count are read from device memory (a wave built on the GPU).
+// Persistent form: arguments and tile count are read from device memory (a wave built on the
+// GPU); blocks take tiles from a shared counter (`next`, zero at launch), so a block that
+// drew light tiles takes more.
 __global__ void __launch_bounds__(256, 4) k_count_lop3_persistent(const CountArgs* __restrict__ args,
-                                                               const int32_t* n_tiles) {
+                                                               const int32_t* n_tiles, int32_t* next) {
     __shared__ Lop3Shared sh;
+    __shared__ int32_t s_t;
     const CountArgs a = *args;
     const int32_t n = *n_tiles;
-    for (int32_t t = blockIdx.x; t < n; t += gridDim.x) lop3_tile(a, a.tiles[t], sh);
+    while (true) {
+        if (threadIdx.x == 0) s_t = atomicAdd(next, 1);
+        __syncthreads();
+        const int32_t t = s_t;
+        __syncthreads();
+        if (t >= n) break;
+        lop3_tile(a, a.tiles[t], sh);
+    }
 }
 
 // masks[dst] = (src >= 0 ? masks[src] : ~0) & AND of the listed item rows.
@@ -276,8 +286,9 @@ int occupancy_lop3(int* blocks) {
     return TFIM_OK;
 }
 
-int launch_count_lop3_persistent(const CountArgs* d_args, const int32_t* d_n_tiles, int32_t grid, cudaStream_t s) {
-    k_count_lop3_persistent<<<grid, 256, 0, s>>>(d_args, d_n_tiles);
+int launch_count_lop3_persistent(const CountArgs* d_args, const int32_t* d_n_tiles, int32_t* d_next, int32_t grid,
+                                 cudaStream_t s) {
+    k_count_lop3_persistent<<<grid, 256, 0, s>>>(d_args, d_n_tiles, d_next);
     TFIM_CUDA(cudaGetLastError());
     return TFIM_OK;
 }

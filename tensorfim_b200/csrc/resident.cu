@@ -65,7 +65,7 @@ struct ResStatus {
     // g_* fields hold its size, for the host to grow the pools and pack again
     int32_t grow, g_rows, g_jobs, g_max_head, g_max_cols, waves;
     int64_t g_out, g_tiles;
-    int32_t launch_id, pad1;
+    int32_t launch_id, next3, next1, pad1;   // next3 / next1: tile counters of the persistent counters
     unsigned long long launch_t0, count_t0;
     unsigned long long supports, nodes, lookaheads, hits, skipped, pep, bytes_alg, count_ns;
 };
@@ -1134,7 +1134,11 @@ __global__ void __launch_bounds__(256) k_top_summary(const int32_t* __restrict__
 __global__ void __launch_bounds__(256) k_res_zero(const ResArgs* __restrict__ args) {
     ResStatus* st = args->p.st;
     int32_t* counts = args->p.counts;
-    if (blockIdx.x == 0 && threadIdx.x == 0) st->count_t0 = globaltimer();
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        st->count_t0 = globaltimer();
+        st->next3 = 0;
+        st->next1 = 0;
+    }
     const int64_t n = st->out_total;
     const int64_t n4 = n >> 2;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -1227,8 +1231,10 @@ int build_wave_graph(WaveGraph& G, const ResArgs* d_args, ResStatus* d_status, b
     do {
         k_res_pack_g<<<1, kPackThreads, 0, s>>>(d_args);
         k_res_zero<<<sm * 4, 256, 0, s>>>(d_args);
-        if ((rc = launch_count_lop3_persistent(&d_args->a3, &d_status->tiles_l3, sm * std::max(1, occ3), s))) break;
-        if ((rc = launch_count_b1_persistent(&d_args->a1, &d_status->tiles_b1, sm * std::max(1, occ1), s))) break;
+        if ((rc = launch_count_lop3_persistent(&d_args->a3, &d_status->tiles_l3, &d_status->next3, sm * std::max(1, occ3), s)))
+            break;
+        if ((rc = launch_count_b1_persistent(&d_args->a1, &d_status->tiles_b1, &d_status->next1, sm * std::max(1, occ1), s)))
+            break;
         if (with_proj &&
             (rc = launch_count_proj_persistent(&d_args->a3, &d_status->n_proj, sm * std::max(1, occp), red_off, red_items, s)))
             break;

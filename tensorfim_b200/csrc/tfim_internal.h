@@ -144,8 +144,10 @@ int launch_count_b1(const CountArgs& a, cudaStream_t s);
 // Persistent forms for waves built on the GPU: the arguments and the tile / job count are
 // read from device memory and a fixed grid strides over the tiles, so the launches do not
 // depend on the wave and can be captured once in a graph.
-int launch_count_lop3_persistent(const CountArgs* d_args, const int32_t* d_n_tiles, int32_t grid, cudaStream_t s);
-int launch_count_b1_persistent(const CountArgs* d_args, const int32_t* d_n_tiles, int32_t grid, cudaStream_t s);
+int launch_count_lop3_persistent(const CountArgs* d_args, const int32_t* d_n_tiles, int32_t* d_next, int32_t grid,
+                                 cudaStream_t s);
+int launch_count_b1_persistent(const CountArgs* d_args, const int32_t* d_n_tiles, int32_t* d_next, int32_t grid,
+                               cudaStream_t s);
 int launch_count_proj_persistent(const CountArgs* d_args, const int32_t* d_n_jobs, int32_t grid, const int64_t* red_off,
                                  const int32_t* red_items, cudaStream_t s);
 // blocks of each persistent kernel resident per SM
