@@ -54,6 +54,8 @@ struct DJob {
     int32_t fam, kind, r0, nr, slot, log;
     int32_t b3, b1;            // exclusive prefix of CUDA-core / tensor-core tiles over the wave's jobs
     int32_t cls, sl3;          // counter (0 CUDA-core, 1 tensor-core, 2 projected); word slices of its CUDA-core tiles
+    int32_t b3l, heavy;        // CUDA-core tiles: heavy jobs' tiles come first (prefix b3), then the light
+                               // jobs' (prefix b3l after all heavy tiles)
 };
 
 struct ResStatus {
@@ -207,12 +209,15 @@ __device__ __forceinline__ int find_job_by_row(const JobDesc* jobs, int nj, int3
     }
     return lo;
 }
-template <bool B1>
+// The last job whose prefix (0: b3, 1: b1, 2: b3l) is <= t: the job owning tile t, since a
+// job with no tiles of that kind shares its prefix with the next job that has some.
+template <int K>
 __device__ __forceinline__ int find_job_by_tile(const DJob* dj, int nj, int64_t t) {
     int lo = 0, hi = nj - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
-        if ((B1 ? dj[mid].b1 : dj[mid].b3) <= t) lo = mid; else hi = mid - 1;
+        const int32_t v = K == 0 ? dj[mid].b3 : K == 1 ? dj[mid].b1 : dj[mid].b3l;
+        if (v <= t) lo = mid; else hi = mid - 1;
     }
     return lo;
 }
@@ -276,7 +281,7 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
             const DFam f = p.fams[L.fam];
             DJob dj;
             dj.fam = L.fam; dj.kind = kJobLook; dj.r0 = 0; dj.nr = 1; dj.slot = L.slot; dj.log = L.log; dj.b3 = 0; dj.b1 = 0;
-            dj.cls = 0; dj.sl3 = 1;
+            dj.cls = 0; dj.sl3 = 1; dj.b3l = 0; dj.heavy = 0;
             p.djobs[k] = dj;
             JobDesc jd;
             jd.base_slot = -1; jd.base_item = -1; jd.n_rows = 1; jd.n_cols = f.nF - f.nT + 1;
@@ -380,7 +385,7 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
             const int32_t jid = s_n_jobs + (int32_t)hx[q];
             DJob dj;
             dj.fam = fid; dj.kind = kJobFam; dj.r0 = f.next_row; dj.nr = take[q]; dj.slot = -1; dj.log = -1; dj.b3 = 0; dj.b1 = 0;
-            dj.cls = 0; dj.sl3 = 1;
+            dj.cls = 0; dj.sl3 = 1; dj.b3l = 0; dj.heavy = 0;
             p.djobs[jid] = dj;
             JobDesc jd;
             jd.base_slot = f.slot; jd.base_item = f.item; jd.n_rows = take[q]; jd.n_cols = f.nF;
@@ -481,34 +486,47 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
     // about 8 tile slices per SM: two rounds of the 4 resident blocks
     const float target = fmaxf(s_cost / (p.l3_slices_per_sm * (float)p.sm_count), 1.f);
     const int64_t max_sl = lmax(1, W / 256);
-    int64_t tot3 = 0;
+    // heavy jobs (cost at least half the slice target) first, so that the longest tiles are
+    // dispatched first and the light ones fill in behind them
+    int64_t tot3h = 0, tot3l = 0;
     for (int base = 0; base < nj; base += kPackCand) {
-        int64_t a3[kPackItems], x3[kPackItems];
+        int64_t ah[kPackItems], al[kPackItems], xh[kPackItems], xl[kPackItems];
         for (int q = 0; q < kPackItems; q++) {
             const int j = base + tid * kPackItems + q;
-            a3[q] = 0;
+            ah[q] = al[q] = 0;
             if (j < nj) {
                 const JobDesc jd = p.jobs[j];
                 DJob* djp = p.djobs + j;
                 if (djp->cls == 0) {
-                    int64_t sl = lmin(max_sl, lmax(1, (int64_t)ceilf(l3_cost(jd, *djp) / target)));
+                    const float cost = l3_cost(jd, *djp);
+                    int64_t sl = lmin(max_sl, lmax(1, (int64_t)ceilf(cost / target)));
                     const int64_t wsl = ((W / 64 + sl - 1) / sl) * 64;
                     sl = wsl > 0 ? (W + wsl - 1) / wsl : 1;
                     djp->sl3 = (int32_t)sl;
-                    a3[q] = l3_tiles(jd.n_rows, jd.n_cols) * sl;
+                    djp->heavy = cost >= 0.5f * target ? 1 : 0;
+                    if (djp->heavy) ah[q] = l3_tiles(jd.n_rows, jd.n_cols) * sl;
+                    else al[q] = l3_tiles(jd.n_rows, jd.n_cols) * sl;
                 }
             }
         }
-        Scan(tmp.scan).ExclusiveSum(a3, x3, s_agg);
+        Scan(tmp.scan).ExclusiveSum(ah, xh, s_agg);
         __syncthreads();
-        const int64_t g3 = s_agg;
+        const int64_t gh = s_agg;
+        Scan(tmp.scan).ExclusiveSum(al, xl, s_agg);
+        __syncthreads();
+        const int64_t gl = s_agg;
         for (int q = 0; q < kPackItems; q++) {
             const int j = base + tid * kPackItems + q;
-            if (j < nj) p.djobs[j].b3 = (int32_t)(tot3 + x3[q]);
+            if (j < nj) {
+                p.djobs[j].b3 = (int32_t)(tot3h + xh[q]);
+                p.djobs[j].b3l = (int32_t)(tot3l + xl[q]);
+            }
         }
-        tot3 += g3;
+        tot3h += gh;
+        tot3l += gl;
         __syncthreads();
     }
+    const int64_t tot3 = tot3h + tot3l;
     const int64_t want1 = lmax(1, (int64_t)(p.b1_tiles_per_sm * (float)p.sm_count));
     int64_t ks1 = tot1 > 0 ? lmax(1, (want1 + tot1 - 1) / tot1) : 1;
     ks1 = lmin(ks1, lmax(1, W / 64));
@@ -545,10 +563,11 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
     }
     if (T3 <= p.cap_tiles)
         for (int64_t t = tid; t < T3; t += kPackThreads) {
-            const int j = find_job_by_tile<false>(p.djobs, nj, t);
+            const bool hv = t < tot3h;
+            const int j = hv ? find_job_by_tile<0>(p.djobs, nj, t) : find_job_by_tile<2>(p.djobs, nj, t - tot3h);
             const JobDesc jd = p.jobs[j];
             const DJob dj = p.djobs[j];
-            const int64_t local = t - dj.b3;
+            const int64_t local = hv ? t - dj.b3 : t - tot3h - dj.b3l;
             const int64_t bt = l3_tiles(jd.n_rows, jd.n_cols);
             const int64_t slice = local / bt, within = local % bt;
             const int64_t wsl = ((W / 64 + dj.sl3 - 1) / dj.sl3) * 64;
@@ -561,7 +580,7 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
     if (T1 <= p.cap_tiles)
         for (int64_t t = tid; t < T1; t += kPackThreads) {
             const int64_t slice = t / tot1, local = t % tot1;
-            const int j = find_job_by_tile<true>(p.djobs, nj, local);
+            const int j = find_job_by_tile<1>(p.djobs, nj, local);
             const JobDesc jd = p.jobs[j];
             const int64_t within = local - p.djobs[j].b1;
             const int cg = (jd.n_cols + kB1Cols - 1) / kB1Cols;
@@ -1403,7 +1422,7 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
         memcpy(at(p_freq), c->dense_freq.data(), c->dense_freq.size() * 4);
         memcpy(at(p_fam), &top, sizeof top);
         memcpy(at(p_F), F0.data(), (size_t)n0 * 4);
-        *(DJob*)at(p_dj) = DJob{0, kJobFam, 0, n0, -1, -1, 0, 0, 0, 1};
+        *(DJob*)at(p_dj) = DJob{0, kJobFam, 0, n0, -1, -1, 0, 0, 0, 1, 0, 0};
         *(JobDesc*)at(p_jd) = JobDesc{-1, -1, n0, n0, 0, 0, 0, -1, 0};
         RowDesc* rows = (RowDesc*)at(p_rows);
         int32_t* rj = (int32_t*)at(p_rj);
