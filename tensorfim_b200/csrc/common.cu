@@ -266,7 +266,7 @@ const char* tfim_last_error(void) { return tfim::get_error(); }
 void tfim_mine_opts_default(tfim_mine_opts* o) {
     if (!o) return;
     memset(o, 0, sizeof *o);
-    o->engine = TFIM_ENGINE_BATCHED;
+    o->engine = TFIM_ENGINE_RESIDENT;
     o->counter = TFIM_COUNTER_AUTO;
     o->wave_cap = 0;
     o->lookahead = 1;

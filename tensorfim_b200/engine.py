@@ -212,7 +212,7 @@ class Database:
             lib().tfim_lookahead_log(self._h, _ptr(x), _ptr(y), n)
         return x, y
 
-    def mine(self, engine: str = "batched", counter: str = "auto", lookahead=True,
+    def mine(self, engine: str = "resident", counter: str = "auto", lookahead=True,
              wave_cap: int = 0, top: str = "auto", log_lookahead: bool = False, proj_auto: int = -1,
              graphs: bool = False, small_pools: bool = False) -> MineResult:
         """lookahead: False/"off", True/"filtered" (every node passing the exact tail-pair
@@ -271,11 +271,11 @@ def result_path(path: str, minsup: float) -> str:
     return "%s-%f=Results.txt" % (path, minsup)
 
 
-def mine_file(path: str, minsup: float, engine: str = "batched", counter: str = "auto", lookahead: int = 1,
-              timeout: float | None = None) -> subprocess.CompletedProcess:
+def mine_file(path: str, minsup: float, engine: str = "resident", counter: str = "auto", lookahead: int = 1,
+              timeout: float | None = None, graphs: bool = False) -> subprocess.CompletedProcess:
     """Run the `tfim` command-line engine exactly as a driver runs the reference's exe."""
     if not os.path.exists(_lib.CLI_PATH):
         raise TfimError(-1, f"{_lib.CLI_PATH} is missing: build it with `python -m tensorfim_b200.build`")
     cmd = [_lib.CLI_PATH, path, repr(float(minsup)), "--engine", engine, "--counter", counter,
-           "--lookahead", str(int(lookahead))]
+           "--lookahead", str(int(lookahead)), "--graphs", str(int(bool(graphs)))]
     return subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)

@@ -115,7 +115,7 @@ def test_cfg4_scaled_matches_oracle(oracle_mod, tmp_path):
 def test_cfg4_full_size_certified():
     db0 = synth.generate(4)
     with tf.Database.from_csr(db0.offsets, db0.items, 0.0005) as db:
-        res = db.mine()
+        res = db.mine(engine="batched")
         assert len(res.mfis) > 1000
         _certify(db, res.mfis, db.dense_to_orig())
         assert db.mine(engine="resident").as_dict() == res.as_dict()
