@@ -15,6 +15,8 @@
 // a2/a3 = the same rows for k 128..255 (g = lane/4, tg = lane%4).  B column-major
 // 256x8: b0 = column g, bits [32*tg, +32) of k 0..127; b1 = the same for k 128..255.
 // C: c0,c1 = row g, columns 2*tg, 2*tg+1; c2,c3 = row g+8.
+#include <atomic>
+
 #include "tfim_internal.h"
 
 namespace tfim {
@@ -232,14 +234,14 @@ __global__ void __launch_bounds__(256) k_count_b1_persistent(const CountArgs* __
 
 int configure_count_kernels() {
     // dynamic shared memory above 48 KiB is opted into once per device
-    static bool done[64] = {};
+    static std::atomic<bool> done[64];
     int dev = 0;
     TFIM_CUDA(cudaGetDevice(&dev));
-    if (dev >= 0 && dev < 64 && done[dev]) return TFIM_OK;
+    if (dev >= 0 && dev < 64 && done[dev].load()) return TFIM_OK;
     const size_t smem = (size_t)kStages * kStageBytes;
     TFIM_CUDA(cudaFuncSetAttribute(k_count_b1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     TFIM_CUDA(cudaFuncSetAttribute(k_count_b1_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    if (dev >= 0 && dev < 64) done[dev] = true;
+    if (dev >= 0 && dev < 64) done[dev].store(true);
     return TFIM_OK;
 }
 

@@ -21,6 +21,8 @@
 //
 // Every mbarrier wait is bounded; on expiry the kernel records an error, stops issuing, and
 // frees its tensor memory.
+#include <atomic>
+
 #include "tfim_internal.h"
 
 namespace tfim {
@@ -286,12 +288,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_count_i8(CountArgs a) {
 
 int launch_count_i8(const CountArgs& a, cudaStream_t s) {
     if (a.n_tiles <= 0) return TFIM_OK;
-    static bool configured[64] = {};
+    static std::atomic<bool> configured[64];
     int dev = 0;
     TFIM_CUDA(cudaGetDevice(&dev));
-    if (dev >= 0 && dev < 64 && !configured[dev]) {
+    if (dev >= 0 && dev < 64 && !configured[dev].load()) {
         TFIM_CUDA(cudaFuncSetAttribute(k_count_i8, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
-        configured[dev] = true;
+        configured[dev].store(true);
     }
     k_count_i8<<<a.n_tiles, kTcThreads, kTcSmem, s>>>(a);
     TFIM_CUDA(cudaGetLastError());

@@ -17,6 +17,8 @@
 #include <cmath>
 #include <numeric>
 
+#include <atomic>
+
 #include "tfim_internal.h"
 
 namespace tfim {
@@ -283,12 +285,12 @@ int ingest_csr(tfim_ctx* c, const int64_t* h_off, const int32_t* h_items, int64_
         if (nnz > 0 && bins <= kHistSmemBins) {
             const int32_t parts = (int32_t)std::min<int64_t>(148, (nnz + 65535) / 65536);
             if ((rc = d_tmp.reserve((size_t)parts * bins * 4))) return done(rc);
-            static bool configured[64] = {};
+            static std::atomic<bool> configured[64];
             int dev = 0;
             cudaGetDevice(&dev);
-            if (dev >= 0 && dev < 64 && !configured[dev]) {
+            if (dev >= 0 && dev < 64 && !configured[dev].load()) {
                 cudaFuncSetAttribute(k_hist_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, kHistSmemBins * 4);
-                configured[dev] = true;
+                configured[dev].store(true);
             }
             k_hist_smem<<<parts, 1024, (size_t)bins * 4, s>>>(d_items.as<int32_t>(), nnz, bins, d_tmp.as<int32_t>());
             k_hist_sum<<<(bins + 255) / 256, 256, 0, s>>>(d_tmp.as<int32_t>(), parts, bins, d_freq.as<int32_t>());

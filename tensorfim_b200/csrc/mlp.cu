@@ -16,6 +16,8 @@
 #include <cstring>
 #include <vector>
 
+#include <atomic>
+
 #include "tfim_internal.h"
 
 namespace tfim {
@@ -196,11 +198,13 @@ int mlp_grad_device(Mlp* m, const float* d_x, const float* d_y, int64_t n, float
                     cudaStream_t s) {
     TFIM_CUDA(cudaMemsetAsync(m->d_grads, 0, sizeof(float) * kMlpParams, s));
     if (n <= 0) return TFIM_OK;
-    static bool configured = false;
+    static std::atomic<bool> configured[64];   // the attribute is per device
     const size_t smem = backward_smem();
-    if (!configured) {
+    int dev = 0;
+    TFIM_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64 || !configured[dev].load()) {
         TFIM_CUDA(cudaFuncSetAttribute(k_mlp_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        configured = true;
+        if (dev >= 0 && dev < 64) configured[dev].store(true);
     }
     k_mlp_backward<<<(unsigned)((n + kBlk - 1) / kBlk), kBlk, smem, s>>>(d_x, d_y, n, m->d_wbf, m->d_params, pos_weight,
                                                                         1.0f / (float)n, m->d_grads, d_loss);
