@@ -253,6 +253,22 @@ TFIM_API int64_t tfim_mfi_item_total(const tfim_ctx* ctx);
 TFIM_API int tfim_get_mfis(const tfim_ctx* ctx, int32_t* items, int64_t* offsets, int32_t* supports);
 
 /*
+ * All frequent itemsets of up to max_len items (supports >= min_count), level by level on the
+ * counting contract: no counterpart in the reference's engines; it restates the reference's
+ * level-wise prototype code/batch_proto/batch_proto.cu:257-409 (every frequent (k-1)-itemset
+ * is a prefix counted against all items; extensions beyond its last item give the frequent
+ * k-itemsets).  Counted items only (a parked id 0 is never a candidate); singleton supports
+ * are bitmap popcounts.  Fails with TFIM_E_NOMEM, keeping nothing, when more than
+ * max_itemsets are frequent.  stats (optional): waves, prefixes counted (nodes), supports.
+ */
+TFIM_API int tfim_mine_all(tfim_ctx* ctx, int32_t min_count, int32_t max_len, int64_t max_itemsets,
+                           tfim_mine_stats* stats);
+TFIM_API int64_t tfim_num_all(const tfim_ctx* ctx);
+TFIM_API int64_t tfim_all_item_total(const tfim_ctx* ctx);
+/* Itemsets by level, then in prefix order; items in ORIGINAL ids, ascending dense order. */
+TFIM_API int tfim_get_all(const tfim_ctx* ctx, int32_t* items, int64_t* offsets, int32_t* supports);
+
+/*
  * Write the reference's results file (code/engine/src/kernel_bitmap.cu:651-690):
  * header keys, "<i>th: <k> { ids }   support: <s>  frequency: <f>" lines, MFIsNumber.
  */

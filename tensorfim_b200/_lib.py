@@ -40,6 +40,7 @@ EXPORTS = [
     "tfim_mlp_create", "tfim_mlp_num_params", "tfim_mlp_set_params", "tfim_mlp_get_params", "tfim_mlp_predict",
     "tfim_mlp_grad", "tfim_mlp_train", "tfim_mlp_free", "tfim_set_proposal", "tfim_lookahead_log",
     "tfim_tuning_get", "tfim_tuning_set", "tfim_tuning_load", "tfim_tuning_source",
+    "tfim_mine_all", "tfim_num_all", "tfim_all_item_total", "tfim_get_all",
 ]
 
 
@@ -146,6 +147,12 @@ def lib() -> C.CDLL:
     L.tfim_tuning_set.argtypes = [P(Tuning)]
     L.tfim_tuning_load.argtypes = [C.c_char_p]
     L.tfim_tuning_source.restype = C.c_char_p
+    L.tfim_mine_all.argtypes = [p, i32, i32, i64, P(MineStats)]
+    L.tfim_num_all.argtypes = [p]
+    L.tfim_num_all.restype = i64
+    L.tfim_all_item_total.argtypes = [p]
+    L.tfim_all_item_total.restype = i64
+    L.tfim_get_all.argtypes = [p, p, p, p]
     for name in EXPORTS:
         getattr(L, name)   # raises AttributeError if an export is missing
     _lib = L

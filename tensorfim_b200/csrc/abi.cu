@@ -44,6 +44,8 @@ int make_ctx(int32_t device, tfim_ctx** out) {
     return TFIM_OK;
 }
 
+}  // namespace
+
 // Per-node masks + one count job over every counted row (the reference counting contract).
 int count_wave_impl(tfim_ctx* c, int32_t b, int32_t min_count, const int32_t* d_items, const MatDesc* d_mats,
                     int32_t* d_counts, int32_t* d_nfreq, cudaStream_t s) {
@@ -129,6 +131,8 @@ int count_wave_impl(tfim_ctx* c, int32_t b, int32_t min_count, const int32_t* d_
     TFIM_CUDA(cudaStreamSynchronize(s));
     return TFIM_OK;
 }
+
+namespace {
 
 __global__ void k_mats_from_offsets(const int64_t* __restrict__ off, int32_t b, MatDesc* __restrict__ mats) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;

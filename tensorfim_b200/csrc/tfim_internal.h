@@ -234,6 +234,8 @@ struct tfim_ctx {
     int64_t mask_slots = 0;
     // results
     tfim::MfiSet mfis;                      // dense ids
+    tfim::MfiSet all_fis;                   // all frequent itemsets of tfim_mine_all (dense ids)
+    bool all_mined = false;
     bool mined = false;
     int32_t counter_pref = TFIM_COUNTER_AUTO;   // counter used by tfim_count_wave
     bool used_i8 = false;                       // the last counting wave ran the tcgen05 i8 counter
@@ -264,4 +266,8 @@ int mine_plain_roots(tfim_ctx* ctx, const std::vector<int32_t>& roots, tfim_mine
 void free_resident(ResidentState* r, cudaStream_t s);
 int mlp_device_params(tfim_mlp* h, const void** wbf, const float** params);
 int compute_bit_supports(tfim_ctx* ctx);
+// Per-node prefix masks from item lists and one count job over every counted row (abi.cu):
+// counts[i][e] = popc(AND of node i's items & B[e]), nfreq[i] = #{e : counts >= min_count}.
+int count_wave_impl(tfim_ctx* c, int32_t b, int32_t min_count, const int32_t* d_items, const MatDesc* d_mats,
+                    int32_t* d_counts, int32_t* d_nfreq, cudaStream_t s);
 }  // namespace tfim

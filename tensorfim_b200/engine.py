@@ -244,6 +244,22 @@ class Database:
         check(lib().tfim_get_mfis(self._h, _ptr(items), _ptr(offs), _ptr(sup)))
         return MineResult(items[:tot], offs, sup[:n], st.as_dict())
 
+    def mine_all(self, min_count: int | None = None, max_len: int = 8, max_itemsets: int = 50_000_000) -> MineResult:
+        """All frequent itemsets of up to max_len items (support >= min_count; default the
+        database's minimum count), level by level on the counting contract -- the reference's
+        level-wise prototype (code/batch_proto/batch_proto.cu).  Items in original ids,
+        in ascending dense-id order; singletons carry their bitmap support."""
+        mc = int(self.info["min_count"] if min_count is None else min_count)
+        st = _lib.MineStats()
+        check(lib().tfim_mine_all(self._h, mc, int(max_len), int(max_itemsets), C.byref(st)))
+        n = lib().tfim_num_all(self._h)
+        tot = lib().tfim_all_item_total(self._h)
+        items = np.zeros(max(tot, 1), dtype=np.int32)
+        offs = np.zeros(n + 1, dtype=np.int64)
+        sup = np.zeros(max(n, 1), dtype=np.int32)
+        check(lib().tfim_get_all(self._h, _ptr(items), _ptr(offs), _ptr(sup)))
+        return MineResult(items[:tot], offs, sup[:n], st.as_dict())
+
     def write_results(self, trans_set_file: str, result_path: str, prep_s: float = 0.0, comp_s: float = 0.0) -> None:
         check(lib().tfim_write_results(self._h, trans_set_file.encode(), result_path.encode(), prep_s, comp_s))
 
