@@ -37,6 +37,7 @@ extern "C" {
 #define TFIM_E_TIMEOUT     5   /* a bounded device-side wait expired */
 #define TFIM_E_STATE       6   /* call order violated (e.g. results before tfim_mine) */
 #define TFIM_E_IO          7   /* results file could not be written */
+#define TFIM_E_COMM        8   /* a sharded context's all-reduce callback reported failure */
 
 typedef struct tfim_ctx tfim_ctx;
 
@@ -97,6 +98,56 @@ TFIM_API int tfim_open_db(const int64_t* row_offsets, const int32_t* items, int6
  */
 TFIM_API int tfim_open_bitmap(const uint32_t* rows, int32_t n_rows, int64_t n_bits, int32_t n_counted,
                      int32_t device, tfim_ctx** out);
+
+/*
+ * Transaction sharding across a process group (one process per GPU).  Each rank holds a
+ * slice of the transactions and opens its context with the group; every per-transaction
+ * statistic the search decides on (id range, row lengths, F1 counts, row supports, wave
+ * counts) is summed (or min/max-reduced) over the group through `allreduce`, so all ranks
+ * see the whole database's numbers, take the same search steps and find the same MFIs.
+ * Integer sums make the result exact.  No counterpart in the reference's engines, which
+ * run on one GPU; this shards a database larger than one GPU's memory by transactions.
+ *
+ * allreduce(buf, count, dtype, op, stream, user): reduce `count` elements at device address
+ * `buf` in place over all ranks (dtype TFIM_DT_*, op TFIM_RED_*), ordered on `stream` (a
+ * cudaStream_t): work enqueued on `stream` after the call returns must see the result.
+ * Return 0 on success.  With NCCL:
+ *   ncclAllReduce(buf, buf, count, dtype ? ncclInt64 : ncclInt32,
+ *                 op == TFIM_RED_SUM ? ncclSum : op == TFIM_RED_MIN ? ncclMin : ncclMax,
+ *                 comm, (cudaStream_t)stream)
+ * Every rank calls the library's entry points in the same order with the same arguments
+ * (apart from its own transactions); the library then issues the same sequence of
+ * collectives on every rank.
+ */
+#define TFIM_DT_I32 0
+#define TFIM_DT_I64 1
+#define TFIM_RED_SUM 0
+#define TFIM_RED_MIN 1
+#define TFIM_RED_MAX 2
+typedef int (*tfim_allreduce_fn)(void* buf, int64_t count, int32_t dtype, int32_t op, void* stream, void* user);
+typedef struct {
+    int32_t rank;                 /* this process's index, 0 .. world-1 */
+    int32_t world;                /* number of shards */
+    tfim_allreduce_fn allreduce;  /* required when world > 1 */
+    void* user;                   /* passed to allreduce */
+} tfim_group;
+
+/*
+ * tfim_open_db over this rank's rows of a transaction-sharded database.  The threshold
+ * applies to the total row count over the group; info fields describe the whole database
+ * except words_per_row (this shard's bitmap).  tfim_mine on the context runs the batched or
+ * plain engine (the default for a sharded context is batched; the resident engine keeps its
+ * counts on the device between waves and is refused with TFIM_E_STATE); tfim_count_wave,
+ * tfim_count_wave_device and tfim_mine_all return whole-database counts.
+ */
+TFIM_API int tfim_open_db_sharded(const int64_t* row_offsets, const int32_t* items, int64_t n_rows,
+                                  double support_threshold, int32_t device, const tfim_group* group, tfim_ctx** out);
+/*
+ * tfim_open_bitmap over this rank's transactions (bit columns) of a sharded bitmap; n_bits
+ * is this shard's transaction count (> 0).  Row supports are summed over the group.
+ */
+TFIM_API int tfim_open_bitmap_sharded(const uint32_t* rows, int32_t n_rows, int64_t n_bits, int32_t n_counted,
+                                      int32_t device, const tfim_group* group, tfim_ctx** out);
 
 TFIM_API int tfim_db_info_get(const tfim_ctx* ctx, tfim_db_info* out);
 /* dense id -> original id (n_dense entries) */

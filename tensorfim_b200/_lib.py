@@ -20,6 +20,7 @@ TFIM_E_DEPTH = 4
 TFIM_E_TIMEOUT = 5
 TFIM_E_STATE = 6
 TFIM_E_IO = 7
+TFIM_E_COMM = 8
 
 ENGINE_PLAIN = 0
 ENGINE_BATCHED = 1
@@ -29,6 +30,11 @@ COUNTER_LOP3 = 1
 COUNTER_TENSOR = 2
 COUNTER_PROJ = 3
 COUNTER_I8 = 4
+DT_I32 = 0
+DT_I64 = 1
+RED_SUM = 0
+RED_MIN = 1
+RED_MAX = 2
 
 # every entry point declared in include/tfim.h
 EXPORTS = [
@@ -36,7 +42,7 @@ EXPORTS = [
     "tfim_dense_to_orig", "tfim_dense_freq", "tfim_count_wave", "tfim_set_counter",
     "tfim_count_wave_device", "tfim_mine_opts_default", "tfim_mine", "tfim_num_mfis",
     "tfim_mfi_item_total", "tfim_get_mfis", "tfim_write_results", "tfim_close",
-    "tfim_count_wave_noalloc",
+    "tfim_count_wave_noalloc", "tfim_open_db_sharded", "tfim_open_bitmap_sharded",
     "tfim_mlp_create", "tfim_mlp_num_params", "tfim_mlp_set_params", "tfim_mlp_get_params", "tfim_mlp_predict",
     "tfim_mlp_grad", "tfim_mlp_train", "tfim_mlp_free", "tfim_set_proposal", "tfim_lookahead_log",
     "tfim_tuning_get", "tfim_tuning_set", "tfim_tuning_load", "tfim_tuning_source",
@@ -81,6 +87,14 @@ class Tuning(C.Structure):
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+# int allreduce(void* buf, int64_t count, int32_t dtype, int32_t op, void* stream, void* user)
+ALLREDUCE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int64, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p)
+
+
+class Group(C.Structure):
+    _fields_ = [("rank", C.c_int32), ("world", C.c_int32), ("allreduce", ALLREDUCE_FN), ("user", C.c_void_p)]
 
 
 class MineStats(C.Structure):
@@ -153,6 +167,8 @@ def lib() -> C.CDLL:
     L.tfim_all_item_total.argtypes = [p]
     L.tfim_all_item_total.restype = i64
     L.tfim_get_all.argtypes = [p, p, p, p]
+    L.tfim_open_db_sharded.argtypes = [p, p, i64, C.c_double, i32, P(Group), P(p)]
+    L.tfim_open_bitmap_sharded.argtypes = [p, i32, i64, i32, i32, P(Group), P(p)]
     for name in EXPORTS:
         getattr(L, name)   # raises AttributeError if an export is missing
     _lib = L

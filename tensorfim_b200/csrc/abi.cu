@@ -40,6 +40,38 @@ int make_ctx(int32_t device, tfim_ctx** out) {
     }
     for (auto& b : c->d_scratch) b.stream = c->stream;
     c->d_masks.stream = c->stream;
+    c->d_group.stream = c->stream;
+    *out = c;
+    return TFIM_OK;
+}
+
+// A context of a sharded database.  Before the ingest's first collective every rank learns
+// whether any rank rejected its arguments, and that the values in `agree` are equal on all
+// ranks, so a bad call fails everywhere instead of leaving the others waiting.
+int make_sharded_ctx(int32_t device, const tfim_group* g, bool args_ok, const std::vector<int64_t>& agree,
+                     const char* what, tfim_ctx** out) {
+    TFIM_CHECK(out != nullptr, TFIM_E_INVALID, "null output handle");
+    *out = nullptr;
+    TFIM_CHECK(g && g->world >= 1 && g->rank >= 0 && g->rank < g->world && (g->world == 1 || g->allreduce),
+               TFIM_E_INVALID, "%s: invalid tfim_group", what);
+    tfim_ctx* c = nullptr;
+    TFIM_TRY(make_ctx(device, &c));
+    c->group = *g;
+    c->sharded = true;
+    std::vector<int64_t> v(1 + 2 * agree.size());
+    v[0] = args_ok ? 0 : 1;
+    for (size_t i = 0; i < agree.size(); i++) { v[1 + 2 * i] = agree[i]; v[2 + 2 * i] = -agree[i]; }
+    int rc = group_reduce_host(c, v.data(), (int32_t)v.size(), TFIM_RED_MAX);
+    if (rc == TFIM_OK && v[0]) {
+        set_error(args_ok ? "%s: another rank's arguments were rejected" : "%s: invalid arguments", what);
+        rc = TFIM_E_INVALID;
+    }
+    for (size_t i = 0; rc == TFIM_OK && i < agree.size(); i++)
+        if (v[1 + 2 * i] != -v[2 + 2 * i]) {
+            set_error("%s: argument %zu differs across the group", what, i);
+            rc = TFIM_E_INVALID;
+        }
+    if (rc != TFIM_OK) { tfim_close(c); return rc; }
     *out = c;
     return TFIM_OK;
 }
@@ -126,6 +158,7 @@ int count_wave_impl(tfim_ctx* c, int32_t b, int32_t min_count, const int32_t* d_
     a.tiles = (const TileDesc*)(dp + o_tiles); a.n_tiles = (int32_t)tiles.size(); a.out = d_counts;
     c->used_i8 = i8;
     TFIM_TRY(i8 ? launch_count_i8(a, s) : b1 ? launch_count_b1(a, s) : launch_count_lop3(a, s));
+    TFIM_TRY(group_reduce(c, d_counts, (int64_t)b * d, TFIM_DT_I32, TFIM_RED_SUM, s));
     TFIM_TRY(launch_nfreq(d_counts, b, d, min_count, d_nfreq, s));
     // the host staging buffer may be reused by the next call only after this copy ran
     TFIM_CUDA(cudaStreamSynchronize(s));
@@ -186,6 +219,32 @@ int tfim_open_bitmap(const uint32_t* rows, int32_t n_rows, int64_t n_bits, int32
     *out = nullptr;
     tfim_ctx* c = nullptr;
     TFIM_TRY(make_ctx(device, &c));
+    int rc = ingest_bitmap(c, rows, n_rows, n_bits, n_counted);
+    if (rc != TFIM_OK) { tfim_close(c); return rc; }
+    *out = c;
+    return TFIM_OK;
+}
+
+int tfim_open_db_sharded(const int64_t* row_offsets, const int32_t* items, int64_t n_rows, double support_threshold,
+                         int32_t device, const tfim_group* group, tfim_ctx** out) {
+    const bool ok = row_offsets != nullptr && n_rows >= 0 && (n_rows == 0 || row_offsets[0] == 0) &&
+                    (n_rows == 0 || row_offsets[n_rows] >= 0) && (n_rows == 0 || row_offsets[n_rows] == 0 || items != nullptr) &&
+                    support_threshold > 0.0 && support_threshold <= 1.0 && std::isfinite(support_threshold);
+    int64_t thr_bits = 0;
+    memcpy(&thr_bits, &support_threshold, 8);
+    tfim_ctx* c = nullptr;
+    TFIM_TRY(make_sharded_ctx(device, group, ok, {thr_bits}, "tfim_open_db_sharded", &c));
+    int rc = ingest_csr(c, row_offsets, items, n_rows, support_threshold);
+    if (rc != TFIM_OK) { tfim_close(c); return rc; }
+    *out = c;
+    return TFIM_OK;
+}
+
+int tfim_open_bitmap_sharded(const uint32_t* rows, int32_t n_rows, int64_t n_bits, int32_t n_counted, int32_t device,
+                             const tfim_group* group, tfim_ctx** out) {
+    const bool ok = rows != nullptr && n_rows > 0 && n_bits > 0 && n_counted >= 0 && n_counted <= n_rows;
+    tfim_ctx* c = nullptr;
+    TFIM_TRY(make_sharded_ctx(device, group, ok, {n_rows, n_counted}, "tfim_open_bitmap_sharded", &c));
     int rc = ingest_bitmap(c, rows, n_rows, n_bits, n_counted);
     if (rc != TFIM_OK) { tfim_close(c); return rc; }
     *out = c;
@@ -285,7 +344,15 @@ int tfim_mine(tfim_ctx* c, const tfim_mine_opts* opts, tfim_mine_stats* stats) {
     TFIM_CUDA(cudaSetDevice(c->device));
     tfim_mine_opts o;
     if (opts) o = *opts;
-    else tfim_mine_opts_default(&o);
+    else {
+        tfim_mine_opts_default(&o);
+        if (c->sharded) o.engine = TFIM_ENGINE_BATCHED;
+    }
+    TFIM_CHECK(o.engine == TFIM_ENGINE_PLAIN || o.engine == TFIM_ENGINE_BATCHED || o.engine == TFIM_ENGINE_RESIDENT,
+               TFIM_E_INVALID, "unknown engine %d", o.engine);
+    TFIM_CHECK(!(c->sharded && o.engine == TFIM_ENGINE_RESIDENT), TFIM_E_STATE,
+               "the resident engine keeps its counts on the device between waves and does not run on a "
+               "transaction-sharded context: use the batched or plain engine");
     tfim_mine_stats st;
     memset(&st, 0, sizeof st);
     c->mfis.clear();
@@ -298,8 +365,7 @@ int tfim_mine(tfim_ctx* c, const tfim_mine_opts* opts, tfim_mine_stats* stats) {
     int rc;
     if (o.engine == TFIM_ENGINE_PLAIN) rc = mine_plain(c, &o, &st);
     else if (o.engine == TFIM_ENGINE_BATCHED) rc = mine_batched(c, &o, &st);
-    else if (o.engine == TFIM_ENGINE_RESIDENT) rc = mine_resident(c, &o, &st);
-    else { set_error("unknown engine %d", o.engine); return TFIM_E_INVALID; }
+    else rc = mine_resident(c, &o, &st);
     cudaEventRecord(e_end, c->stream);
     cudaEventSynchronize(e_end);
     const auto t1 = std::chrono::steady_clock::now();
@@ -457,6 +523,7 @@ void tfim_close(tfim_ctx* c) {
     for (auto& b : c->d_scratch) b.release();
     for (auto& b : c->h_scratch) b.release();
     c->d_masks.release();
+    c->d_group.release();
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);

@@ -234,10 +234,21 @@ int compute_bit_supports(tfim_ctx* c) {
         TFIM_CUDA(cudaMemcpyAsync(all.data(), c->d_scratch[7].p, (size_t)rows * 4, cudaMemcpyDeviceToHost, c->stream));
         TFIM_CUDA(cudaStreamSynchronize(c->stream));
     }
-    c->bit_support.assign(all.begin(), all.begin() + std::min<int32_t>(rows, c->n_counted));
     int64_t total = 0;
     for (int32_t v : all) total += v;
     c->csr_exact = c->from_db && c->d_red_off && total == c->n_red_items;
+    if (c->sharded) {
+        // row supports summed over the shards; the list counters are exact only if every shard's list is
+        if (rows > 0) {
+            TFIM_TRY(group_reduce(c, c->d_scratch[7].p, rows, TFIM_DT_I32, TFIM_RED_SUM, c->stream));
+            TFIM_CUDA(cudaMemcpyAsync(all.data(), c->d_scratch[7].p, (size_t)rows * 4, cudaMemcpyDeviceToHost, c->stream));
+            TFIM_CUDA(cudaStreamSynchronize(c->stream));
+        }
+        int64_t inexact = c->csr_exact ? 0 : 1;
+        TFIM_TRY(group_reduce_host(c, &inexact, 1, TFIM_RED_MAX));
+        c->csr_exact = inexact == 0;
+    }
+    c->bit_support.assign(all.begin(), all.begin() + std::min<int32_t>(rows, c->n_counted));
     return TFIM_OK;
 }
 
@@ -274,9 +285,26 @@ int ingest_csr(tfim_ctx* c, const int64_t* h_off, const int32_t* h_items, int64_
     if (n_rows > 0) k_row_lengths<<<grid_for(n_rows), 256, 0, s>>>(d_off.as<int64_t>(), n_rows, d_stats.as<ScanStats>());
     cudaMemcpyAsync(&hs, d_stats.p, sizeof hs, cudaMemcpyDeviceToHost, s);
     if (cudaStreamSynchronize(s) != cudaSuccess) { set_error("ingest statistics pass failed: %s", cudaGetErrorString(cudaGetLastError())); return done(TFIM_E_CUDA); }
+    int64_t n_rows_all = n_rows;
+    if (c->sharded) {
+        // the whole database's statistics: errors, id range and row lengths (MIN as -MAX(-x))
+        int64_t mx[6] = {hs.neg, hs.bad_off, nnz > 0 ? (int64_t)hs.id_max : -1, n_rows > 0 ? (int64_t)hs.len_max : 0,
+                         nnz > 0 ? -(int64_t)hs.id_min : -(int64_t)INT_MAX, n_rows > 0 ? -(int64_t)hs.len_min : -(int64_t)LLONG_MAX};
+        int64_t sm[3] = {n_rows, (int64_t)hs.len_sum, nnz};
+        if ((rc = group_reduce_host(c, mx, 6, TFIM_RED_MAX)) || (rc = group_reduce_host(c, sm, 3, TFIM_RED_SUM))) return done(rc);
+        hs.neg = (int32_t)mx[0];
+        hs.bad_off = (int32_t)mx[1];
+        n_rows_all = sm[0];
+        hs.len_sum = (unsigned long long)sm[1];
+        if (sm[2] > 0) { id_max = mx[2]; id_min = -mx[4]; }
+        hs.len_max = mx[3];
+        hs.len_min = -mx[5];
+    } else if (nnz > 0) {
+        id_min = hs.id_min;
+        id_max = hs.id_max;
+    }
     if (hs.neg) { set_error("negative item id in the transaction set"); return done(TFIM_E_INVALID); }
     if (hs.bad_off) { set_error("row_offsets must be non-decreasing"); return done(TFIM_E_INVALID); }
-    if (nnz > 0) { id_min = hs.id_min; id_max = hs.id_max; }
 
     // F1 histogram over ids 0..id_max (kernel_bitmap.cu:269-275)
     if ((rc = d_freq.reserve((size_t)(id_max + 1) * 4))) return done(rc);
@@ -299,28 +327,29 @@ int ingest_csr(tfim_ctx* c, const int64_t* h_off, const int32_t* h_items, int64_
             if (nnz > 0) k_hist<<<grid_for(nnz), 256, 0, s>>>(d_items.as<int32_t>(), nnz, d_freq.as<int32_t>());
         }
     }
+    if ((rc = group_reduce(c, d_freq.p, id_max + 1, TFIM_DT_I32, TFIM_RED_SUM, s))) return done(rc);
     freq.assign((size_t)id_max + 1, 0);
     cudaMemcpyAsync(freq.data(), d_freq.p, (size_t)(id_max + 1) * 4, cudaMemcpyDeviceToHost, s);
     if (cudaStreamSynchronize(s) != cudaSuccess) { set_error("F1 histogram failed: %s", cudaGetErrorString(cudaGetLastError())); return done(TFIM_E_CUDA); }
 
     tfim_db_info& I = c->info;
     memset(&I, 0, sizeof I);
-    I.trans_num = n_rows;
+    I.trans_num = n_rows_all;
     I.item_id_min = id_min;
     I.item_id_max = id_max;
-    I.trans_len_min = n_rows > 0 ? hs.len_min : INT_MAX;
-    I.trans_len_max = n_rows > 0 ? hs.len_max : 0;
-    I.trans_len_mean = n_rows > 0 ? (double)hs.len_sum / (double)n_rows : 0.0;
+    I.trans_len_min = n_rows_all > 0 ? hs.len_min : INT_MAX;
+    I.trans_len_max = n_rows_all > 0 ? hs.len_max : 0;
+    I.trans_len_mean = n_rows_all > 0 ? (double)hs.len_sum / (double)n_rows_all : 0.0;
     int64_t dim = 0;
     for (int64_t i = 0; i <= id_max; i++) dim += freq[i] != 0;
     I.dimension = dim;
     I.support_threshold = thr;
-    const double fthr = (double)n_rows * thr;                 // kernel_bitmap.cu:806
+    const double fthr = (double)n_rows_all * thr;             // kernel_bitmap.cu:806
     I.frequency_threshold = fthr;
     I.min_count = (int32_t)std::max(0.0, std::ceil(fthr));     // v >= fthr  <=>  v >= ceil(fthr) for integer v
     int64_t dimred = 0;
     for (int64_t i = 0; i <= id_max; i++)                       // kernel_bitmap.cu:815-816
-        if ((double)freq[i] / (double)n_rows > thr) dimred++;
+        if ((double)freq[i] / (double)n_rows_all > thr) dimred++;
     I.dimension_reduced = dimred;
 
     // dense ids (kernel_bitmap.cu:348-373)
@@ -380,10 +409,21 @@ int ingest_csr(tfim_ctx* c, const int64_t* h_off, const int32_t* h_items, int64_
         n_red = last[0] + (last_len > 0);
         n_red_items = last[1] + last_len;
     }
-    I.trans_num_reduced = n_red;
-    I.trans_len_red_min = n_red > 0 ? hs.red_min : INT_MAX;
-    I.trans_len_red_max = n_red > 0 ? hs.red_max : 0;
-    I.trans_len_red_mean = (double)hs.red_sum / (double)n_red;   // 0/0 -> nan, as the reference
+    int64_t n_red_all = n_red;
+    if (c->sharded) {
+        int64_t mx[2] = {n_red > 0 ? (int64_t)hs.red_max : 0, n_red > 0 ? -(int64_t)hs.red_min : -(int64_t)LLONG_MAX};
+        int64_t sm[3] = {n_red, (int64_t)hs.red_sum, (int64_t)hs.red_sq_sum};
+        if ((rc = group_reduce_host(c, mx, 2, TFIM_RED_MAX)) || (rc = group_reduce_host(c, sm, 3, TFIM_RED_SUM))) return done(rc);
+        hs.red_max = mx[0];
+        hs.red_min = -mx[1];
+        n_red_all = sm[0];
+        hs.red_sum = (unsigned long long)sm[1];
+        hs.red_sq_sum = (unsigned long long)sm[2];
+    }
+    I.trans_num_reduced = n_red_all;
+    I.trans_len_red_min = n_red_all > 0 ? hs.red_min : INT_MAX;
+    I.trans_len_red_max = n_red_all > 0 ? hs.red_max : 0;
+    I.trans_len_red_mean = (double)hs.red_sum / (double)n_red_all;   // 0/0 -> nan, as the reference
     c->red_pair_work = (double)hs.red_sq_sum;
     if ((rc = dev_alloc((void**)&c->d_red_off, (size_t)(n_red + 1) * 8, s)) ||
         (rc = dev_alloc((void**)&c->d_red_items, (size_t)std::max<int64_t>(n_red_items, 1) * 4, s)))
@@ -396,7 +436,9 @@ int ingest_csr(tfim_ctx* c, const int64_t* h_off, const int32_t* h_items, int64_
 
     // the bitmap: n_dense rows x W words, zero padded
     c->n_bits = n_red;
+    c->n_bits_total = n_red_all;
     c->W = words_for_bits(n_red);
+    if (c->sharded && c->W < kRowAlignWords) c->W = kRowAlignWords;   // an empty shard counts zeros
     I.words_per_row = (int32_t)c->W;
     const size_t bm_bytes = (size_t)std::max<int32_t>(n_dense, 1) * (size_t)std::max<int64_t>(c->W, 1) * 4;
     if ((rc = dev_alloc((void**)&c->d_bitmap, bm_bytes, s))) return done(rc);
@@ -417,12 +459,14 @@ int ingest_bitmap(tfim_ctx* c, const uint32_t* rows, int32_t n_rows, int64_t n_b
                "tfim_open_bitmap: invalid arguments");
     const int64_t src_w = (n_bits + 31) / 32;
     c->n_bits = n_bits;
+    c->n_bits_total = n_bits;
+    if (c->sharded) TFIM_TRY(group_reduce_host(c, &c->n_bits_total, 1, TFIM_RED_SUM));
     c->W = words_for_bits(n_bits);
     c->n_counted = n_counted;
     memset(&c->info, 0, sizeof c->info);
     c->info.n_survivors = n_counted;
     c->info.n_dense = n_rows;
-    c->info.trans_num_reduced = n_bits;
+    c->info.trans_num_reduced = c->n_bits_total;
     c->info.words_per_row = (int32_t)c->W;
     const size_t bytes = (size_t)n_rows * (size_t)c->W * 4;
     TFIM_TRY(dev_alloc((void**)&c->d_bitmap, bytes, c->stream));

@@ -292,6 +292,8 @@ struct WaveRunner {
             count_launches++;
         }
         TFIM_CUDA(cudaEventRecord(c->ev1, s));
+        // a transaction-sharded context sums the partial counts of the whole wave over the group
+        TFIM_TRY(group_reduce(c, d_counts.p, w.out_total, TFIM_DT_I32, TFIM_RED_SUM, s));
         if (w.top_job >= 0) {
             const JobDesc& tj = w.jobs[w.top_job];
             TFIM_TRY(launch_mirror(d_counts.as<int32_t>() + tj.out_off, tj.n_rows,
@@ -593,7 +595,7 @@ int mine_batched(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* st) {
         const bool b1 = wr.counter != TFIM_COUNTER_LOP3 &&
                         (wr.counter == TFIM_COUNTER_TENSOR || (nF >= tn.b1_min_rows && nF >= tn.b1_min_cols));
         const double bit_rate = b1 ? tn.rate_b1_bitops : tn.rate_lop3_bitops;
-        const double bitmap_s = nF * nF * (double)c->n_bits / 2.0 / bit_rate;
+        const double bitmap_s = nF * nF * (double)c->n_bits_total / 2.0 / bit_rate;
         const double pairs_s = c->red_pair_work / 2.0 / tn.rate_pair_incr + nF * nF * 4.0 / kTuneHbmBytes;
         if (fits) {
             if (o->top_counter == 1) top_mode = 1;
@@ -793,7 +795,7 @@ int mine_batched(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* st) {
                         cd.src_slot = P.slot;
                         cd.src_item = P.item;
                         cd.t = t;
-                        lookahead_features(cd.feat, (int)ch.head.size(), tail, (int)ch.F.size(), supc, minc, c->n_bits,
+                        lookahead_features(cd.feat, (int)ch.head.size(), tail, (int)ch.F.size(), supc, minc, c->n_bits_total,
                                            (int)eq.size(), pairs ? (double)pairs_ok / (double)pairs : 1.0, nT, i,
                                            P.slot < 0 && P.item < 0);
                         cands.push_back(cd);

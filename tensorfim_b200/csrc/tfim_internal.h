@@ -248,6 +248,12 @@ struct tfim_ctx {
     float proposal_threshold = 0.5f;
     std::vector<float> la_feats;    // n x 32
     std::vector<float> la_labels;   // n
+    // transaction sharding (tfim_open_*_sharded): the group, and the transaction count over
+    // all shards (equal to n_bits for an unsharded context); decisions use the latter
+    tfim_group group{0, 1, nullptr, nullptr};
+    bool sharded = false;
+    int64_t n_bits_total = 0;
+    tfim::DevBuf d_group;                   // staging of host values reduced over the group
 };
 
 namespace tfim {
@@ -270,4 +276,9 @@ int compute_bit_supports(tfim_ctx* ctx);
 // counts[i][e] = popc(AND of node i's items & B[e]), nfreq[i] = #{e : counts >= min_count}.
 int count_wave_impl(tfim_ctx* c, int32_t b, int32_t min_count, const int32_t* d_items, const MatDesc* d_mats,
                     int32_t* d_counts, int32_t* d_nfreq, cudaStream_t s);
+// In-place all-reduce of `count` device elements over a sharded context's group, ordered on
+// `s`; nothing for an unsharded context (shard.cu).
+int group_reduce(tfim_ctx* c, void* d_buf, int64_t count, int32_t dtype, int32_t op, cudaStream_t s);
+// The same for n host int64 values (staged through the context's device buffer).
+int group_reduce_host(tfim_ctx* c, int64_t* vals, int32_t n, int32_t op);
 }  // namespace tfim

@@ -127,10 +127,12 @@ def shipped_proposal(device: int = 0):
 class Database:
     """A transaction database resident on one GPU (a tfim_ctx)."""
 
-    def __init__(self, handle: C.c_void_p, device: int = 0):
+    def __init__(self, handle: C.c_void_p, device: int = 0, group=None):
         self._h = handle
         self._device = device
         self._proposal = None
+        self._group = group   # a sharded context calls back into it: kept alive while open
+        self.sharded = group is not None
         info = _lib.DbInfo()
         check(lib().tfim_db_info_get(self._h, C.byref(info)))
         self.info = info.as_dict()
@@ -155,6 +157,29 @@ class Database:
         h = C.c_void_p()
         check(lib().tfim_open_bitmap(_ptr(rows), rows.shape[0], int(n_bits), int(n_counted), device, C.byref(h)))
         return cls(h, device)
+
+    @classmethod
+    def from_csr_sharded(cls, offsets: np.ndarray, items: np.ndarray, minsup: float, group, device: int = 0) -> "Database":
+        """This shard's rows of a transaction-sharded database (tfim_open_db_sharded); `group` is
+        a tensorfim_b200.shard.Group (TorchGroup, or a ThreadGroup member).  Counts, info and
+        mined sets are the whole database's; every shard must make the same calls."""
+        offsets = np.ascontiguousarray(offsets, dtype=np.int64)
+        items = np.ascontiguousarray(items, dtype=np.int32)
+        g = group.struct()
+        h = C.c_void_p()
+        check(lib().tfim_open_db_sharded(_ptr(offsets), _ptr(items), offsets.shape[0] - 1, float(minsup), device,
+                                         C.byref(g), C.byref(h)))
+        return cls(h, device, group)
+
+    @classmethod
+    def from_bitmap_sharded(cls, rows: np.ndarray, n_bits: int, n_counted: int, group, device: int = 0) -> "Database":
+        """This shard's transactions (bit columns) of a vertical bitmap (tfim_open_bitmap_sharded)."""
+        rows = np.ascontiguousarray(rows, dtype=np.uint32)
+        g = group.struct()
+        h = C.c_void_p()
+        check(lib().tfim_open_bitmap_sharded(_ptr(rows), rows.shape[0], int(n_bits), int(n_counted), device,
+                                             C.byref(g), C.byref(h)))
+        return cls(h, device, group)
 
     # -- tables --------------------------------------------------------------------------
     def dense_to_orig(self) -> np.ndarray:
@@ -212,17 +237,18 @@ class Database:
             lib().tfim_lookahead_log(self._h, _ptr(x), _ptr(y), n)
         return x, y
 
-    def mine(self, engine: str = "resident", counter: str = "auto", lookahead=True,
+    def mine(self, engine: str | None = None, counter: str = "auto", lookahead=True,
              wave_cap: int = 0, top: str = "auto", log_lookahead: bool = False, proj_auto: int = -1,
              graphs: bool = False, small_pools: bool = False) -> MineResult:
         """lookahead: False/"off", True/"filtered" (every node passing the exact tail-pair
         filter), "learned" (the attached proposal, or the shipped weights), "all".
         graphs: (resident engine) run the wave loop as a captured CUDA graph whose conditional
         WHILE node repeats pack -> count -> expand on the device; the host reads the status
-        only when the search ends or a pool has to grow."""
+        only when the search ends or a pool has to grow.
+        engine: "resident" (default), "batched" (default for a sharded database) or "plain"."""
         o = _lib.MineOpts()
         lib().tfim_mine_opts_default(C.byref(o))
-        o.engine = ENGINES[engine]
+        o.engine = ENGINES[engine or ("batched" if self.sharded else "resident")]
         o.counter = COUNTERS[counter]
         la = {False: 0, True: 1, "off": 0, "filtered": 1, "learned": 2, "all": 3}[lookahead]
         if la == 2 and getattr(self, "_proposal", None) is None:
@@ -268,6 +294,7 @@ class Database:
             lib().tfim_close(self._h)
             self._h = None
         self._proposal = None
+        self._group = None
 
     def __enter__(self):
         return self

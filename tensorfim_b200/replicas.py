@@ -1,9 +1,8 @@
 """Replica bookkeeping of the multi-GPU benchmark.
 
-The MFI search of one database does not shard in this build (SURVEY §8e's root-subtree and
-transaction sharding are designs, not built), so `bench.py --gpus N` runs N independent
-replicas: each rank mines its own copy of the database and no collective touches the data
-path.  The only collective is the timing reduction: the job takes as long as its slowest
+The benchmark workloads fit one GPU, so `bench.py --gpus N` runs N independent replicas:
+each rank mines its own copy of the database and no collective touches the data path
+(transaction sharding, tensorfim_b200.shard, is for databases beyond one GPU's memory).  The only collective is the timing reduction: the job takes as long as its slowest
 rank, and its throughput is the supports all ranks counted over that time (weak scaling).
 Works on any torch.distributed backend (NCCL with CUDA tensors on the GPU box, gloo on CPU
 in the tests).
