@@ -226,7 +226,11 @@ typedef struct {
                               counter: -1 tuned default, 0 no, 1 yes */
     int32_t small_pools;   /* resident engine: start from minimal pool capacities so that
                               every pool grows during the search (exercises the growth path) */
-    int32_t reserved[7];
+    int32_t superset;      /* resident engine: 1 drops a family whose head and whole tail lie
+                              inside an MFI already found (none of its itemsets can be a new
+                              maximal set), at creation and again before it leaves the stack;
+                              0 (default) off.  Speed only: the MFI set is the same either way */
+    int32_t reserved[6];
 } tfim_mine_opts;
 
 typedef struct {
@@ -249,6 +253,7 @@ typedef struct {
     double  sync_ms;           /* host time blocked on device results */
     int64_t lookaheads_skipped;/* lookaheads ruled out because a tail pair is infrequent */
     double  top_ms;            /* CUDA-event time of counting the empty-prefix family (resident) */
+    int64_t pruned_superset;   /* families dropped by the superset check (resident) */
 } tfim_mine_stats;
 
 /* ------------------------------------------------------------------ tuning table

@@ -75,7 +75,7 @@ class MineOpts(C.Structure):
     _fields_ = [("engine", C.c_int32), ("counter", C.c_int32), ("wave_cap", C.c_int32),
                 ("lookahead", C.c_int32), ("use_graphs", C.c_int32), ("top_counter", C.c_int32),
                 ("log_lookahead", C.c_int32), ("proj_auto", C.c_int32), ("small_pools", C.c_int32),
-                ("reserved", C.c_int32 * 7)]
+                ("superset", C.c_int32), ("reserved", C.c_int32 * 6)]
 
 
 class Tuning(C.Structure):
@@ -103,7 +103,7 @@ class MineStats(C.Structure):
                 ("waves", C.c_int64), ("launches", C.c_int64), ("count_launches", C.c_int64),
                 ("lookaheads", C.c_int64), ("lookahead_hits", C.c_int64), ("pruned_pep", C.c_int64),
                 ("n_mfi", C.c_int64), ("host_ms", C.c_double), ("sync_ms", C.c_double),
-                ("lookaheads_skipped", C.c_int64), ("top_ms", C.c_double)]
+                ("lookaheads_skipped", C.c_int64), ("top_ms", C.c_double), ("pruned_superset", C.c_int64)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}

@@ -272,6 +272,7 @@ void tfim_mine_opts_default(tfim_mine_opts* o) {
     o->lookahead = 1;
     o->use_graphs = 0;
     o->proj_auto = -1;
+    o->superset = 0;
 }
 
 }  // extern "C"

@@ -70,6 +70,9 @@ struct ResStatus {
     int32_t launch_id, next3, next1, pad1;   // next3 / next1: tile counters of the persistent counters
     unsigned long long launch_t0, count_t0;
     unsigned long long supports, nodes, lookaheads, hits, skipped, pep, bytes_alg, count_ns;
+    // superset check: MFIs [0, sup_done) are in the item -> MFI index the expand reads
+    int32_t sup_done, pad2;
+    unsigned long long sup_pruned;
 };
 
 // Pool capacities, in entries.  A wave is packed only when the worst case of its expand fits.
@@ -140,6 +143,10 @@ struct ResPtrs {
     // graph-driven wave loop: stop after wave_limit waves or max_launch_ns of device time
     int32_t wave_limit, launch_id;
     unsigned long long max_launch_ns;
+    // superset check (nullptr: off): bit k of word sup_index[x * sup_words + k / 32] is set
+    // when MFI k holds item x, for items x < sup_items and MFIs k < sup_words * 32
+    uint32_t* sup_index;
+    int32_t sup_words, sup_items;
 };
 
 // The first pass of the expand over one counted row: extensions (count >= min_count, own
@@ -245,6 +252,8 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
         st->n_mjobs = 0;
         st->grow = 0;
         st->starved = 0;
+        // MFIs of the finished waves are indexed (k_index_mfis ran after the last expand)
+        if (p.sup_index) st->sup_done = min(st->mfi_n, p.sup_words * 32);
         if (st->launch_id != p.launch_id) {
             st->launch_id = p.launch_id;
             st->launch_t0 = globaltimer();
@@ -680,6 +689,28 @@ __device__ void warp_emit_mfi(const ResPtrs& p, const int32_t* head, int head_le
     }
 }
 
+// Whether some indexed MFI (ids below `done`) holds every item of head[0, nh) and tail[0, nt):
+// one index word per lane, ANDed over the items until every lane's word is zero.  Items
+// beyond the index hold no indexed MFI.
+__device__ bool warp_covered(const ResPtrs& p, int32_t done, const int32_t* head, int nh, const int32_t* tail, int nt,
+                             int lane) {
+    const int nw = (done + 31) >> 5;
+    const int n = nh + nt;
+    for (int w0 = 0; w0 < nw; w0 += 32) {
+        const int w = w0 + lane;
+        uint32_t acc = w < nw ? ~0u : 0u;
+        if (w == nw - 1 && (done & 31)) acc = (1u << (done & 31)) - 1u;
+        for (int q = 0; q < n; q++) {
+            if (!__any_sync(0xffffffffu, acc != 0u)) break;
+            const int32_t x = q < nh ? head[q] : tail[q - nh];
+            if (x < 0 || x >= p.sup_items) acc = 0u;
+            else if (acc) acc &= p.sup_index[(int64_t)x * p.sup_words + w];
+        }
+        if (__any_sync(0xffffffffu, acc != 0u)) return true;
+    }
+    return false;
+}
+
 __device__ void finish_row(const ResPtrs& p, DFam* f, int lane) {
     if (lane == 0) {
         const int32_t done = atomicAdd(&f->rows_done, 1) + 1;
@@ -931,6 +962,13 @@ __device__ void expand_row(const ResPtrs& p, int64_t g, int lane) {
         for (int a = lane; a < n_tail; a += 32) Fc[a] = F[stage[a]];
     }
     __syncwarp();
+    // superset check: every itemset of the child's subtree lies inside head' + tail; when an
+    // MFI of an earlier wave holds them all, none of those itemsets is a new maximal set
+    if (p.sup_index && warp_covered(p, p.st->sup_done, hc, head_len, Fc, n_tail, lane)) {
+        if (lane == 0) atomicAdd(&st->sup_pruned, 1ull);
+        finish_row(p, fp, lane);
+        return;
+    }
     // base mask of the child
     int32_t cslot = -1, citem = -1;
     if (f.slot < 0 && f.item < 0) {
@@ -1093,6 +1131,56 @@ __device__ __forceinline__ void build_masks(const ResPtrs& p) {
 }
 __global__ void __launch_bounds__(256) k_build_masks(ResPtrs p) { build_masks(p); }
 
+// Add the MFIs emitted since the last pack to the superset index: one warp per MFI, one
+// atomicOr per item.  An MFI holding an item beyond the index is left out (it then prunes
+// nothing); so are MFIs beyond the index's capacity.
+__device__ void index_mfis(const ResPtrs& p) {
+    if (!p.sup_index) return;
+    const int32_t lo = p.st->sup_done;
+    const int32_t hi = min(p.st->mfi_n, p.sup_words * 32);
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t k = lo + (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / 32; k < hi; k += warps) {
+        const int32_t off = p.mfi_off[k], len = p.mfi_len[k];
+        bool ok = true;
+        for (int q = lane; q < len; q += 32) {
+            const int32_t x = p.mfi_items[off + q];
+            ok &= x >= 0 && x < p.sup_items;
+        }
+        if (!__all_sync(0xffffffffu, ok)) continue;
+        const uint32_t bit = 1u << (k & 31);
+        for (int q = lane; q < len; q += 32)
+            atomicOr(&p.sup_index[(int64_t)p.mfi_items[off + q] * p.sup_words + (k >> 5)], bit);
+    }
+}
+__global__ void __launch_bounds__(256) k_index_mfis(ResPtrs p) { index_mfis(p); }
+
+// Families waiting on the stack that an MFI found since their creation covers: a fresh
+// family (no row handed out, not waiting on a lookahead) whose head and whole tail lie inside
+// an indexed MFI is marked finished and its mask slot released; the pack then pops it without
+// a job.  One warp per stack entry, from the top, over the entries the next waves take first.
+__device__ void prune_stack(const ResPtrs& p) {
+    if (!p.sup_index) return;
+    ResStatus* st = p.st;
+    const int32_t done = min(st->mfi_n, p.sup_words * 32);   // k_index_mfis has indexed these
+    const int32_t n = st->stack_n;
+    const int32_t depth = min(n, 4 * p.wave_rows);
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t k = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / 32; k < depth; k += warps) {
+        const int32_t fid = p.stack[n - 1 - k];
+        DFam* fp = p.fams + fid;
+        const DFam f = *fp;
+        if (f.state != 0 || f.next_row != 0 || f.rows_done != 0 || f.top) continue;
+        if (warp_covered(p, done, p.heads + f.head_off, f.head_len, p.items + f.F_off, f.nT, lane) && lane == 0) {
+            fp->state = 2;
+            release_slot(p, f.slot);
+            atomicAdd(&st->sup_pruned, 1ull);
+        }
+    }
+}
+__global__ void __launch_bounds__(256) k_prune_stack(ResPtrs p) { prune_stack(p); }
+
 // The expand's first pass for the family of the empty prefix (an n x n count block whose
 // rows are its tail, nT = nF = n): one block per row streams the row with four loads in
 // flight per thread and writes the row's summary.
@@ -1181,6 +1269,9 @@ __global__ void __launch_bounds__(256) k_build_masks_g(const ResArgs* __restrict
     build_masks(p);
 }
 
+__global__ void __launch_bounds__(256) k_index_mfis_g(const ResArgs* __restrict__ args) { index_mfis(args->p); }
+__global__ void __launch_bounds__(256) k_prune_stack_g(const ResArgs* __restrict__ args) { prune_stack(args->p); }
+
 __global__ void k_res_control(const ResArgs* __restrict__ args, cudaGraphConditionalHandle h) {
     if (threadIdx.x != 0) return;
     ResStatus* st = args->p.st;
@@ -1259,6 +1350,8 @@ int build_wave_graph(WaveGraph& G, const ResArgs* d_args, ResStatus* d_status, b
             break;
         k_res_expand_g<<<sm * std::max(1, occe), 256, 0, s>>>(d_args);
         k_build_masks_g<<<sm * 8, 256, 0, s>>>(d_args);
+        k_index_mfis_g<<<sm, 256, 0, s>>>(d_args);
+        k_prune_stack_g<<<sm, 256, 0, s>>>(d_args);
         k_res_control<<<1, 32, 0, s>>>(d_args, h);
     } while (0);
     cudaGraph_t captured = nullptr;
@@ -1278,7 +1371,7 @@ int build_wave_graph(WaveGraph& G, const ResArgs* d_args, ResStatus* d_status, b
 struct ResidentState {
     Pool fams, items, heads, stack, looks, free_slots, defer, mfi_off, mfi_len, mfi_sup, mfi_items, log_feat, log_label;
     Pool djobs, jobs, rows, row_job, row_local, tiles_l3, tiles_b1, counts, status, is_root, dense_freq, top_pos, top_diag,
-        proj_list, args, top_sum, mjobs;
+        proj_list, args, top_sum, mjobs, sup_index;
     HostBuf h_status, h_args, h_res, h_setup;
     WaveGraph graph;
     int32_t launch_id = 0;
@@ -1286,7 +1379,8 @@ struct ResidentState {
         graph.release();
         for (Pool* b : {&fams, &items, &heads, &stack, &looks, &free_slots, &defer, &mfi_off, &mfi_len, &mfi_sup, &mfi_items,
                         &log_feat, &log_label, &djobs, &jobs, &rows, &row_job, &row_local, &tiles_l3, &tiles_b1, &counts,
-                        &status, &is_root, &dense_freq, &top_pos, &top_diag, &proj_list, &args, &top_sum, &mjobs}) {
+                        &status, &is_root, &dense_freq, &top_pos, &top_diag, &proj_list, &args, &top_sum, &mjobs,
+                        &sup_index}) {
             dev_free(b->p, s);
             b->p = nullptr;
             b->bytes = 0;
@@ -1380,6 +1474,15 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
     TFIM_TRY(grow(R.dense_freq, (size_t)std::max<int32_t>(c->info.n_dense, 1) * 4, s));
     TFIM_TRY(grow(R.top_pos, (size_t)std::max<int32_t>(c->info.n_dense, 1) * 4, s));
     TFIM_TRY(grow(R.top_diag, (size_t)n0 * 4, s));
+    // superset index (opts.superset): d items x sup_words words (about 32 MiB; MFIs past its
+    // capacity are not indexed and prune nothing), cleared for every mine
+    const bool sup_on = o->superset != 0;
+    const int32_t sup_words = (int32_t)std::min<int64_t>(65536, std::max<int64_t>(32, (8LL << 20) / std::max(d, 1)));
+    if (sup_on) {
+        const size_t sup_bytes = (size_t)d * (size_t)sup_words * 4;
+        TFIM_TRY(grow(R.sup_index, sup_bytes, s));
+        TFIM_CUDA(cudaMemsetAsync(R.sup_index.p, 0, sup_bytes, s));
+    }
     // mask slots (grown on demand)
     int64_t slot_cap = c->d_masks.bytes / ((size_t)W * 4);
 
@@ -1515,6 +1618,9 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
         P.wave_limit = 0x7fffffff;
         P.launch_id = 0;
         P.max_launch_ns = 2000000000ull;
+        P.sup_index = sup_on ? (uint32_t*)R.sup_index.p : nullptr;
+        P.sup_words = sup_words;
+        P.sup_items = d;
     };
     // capacity for the worst case of one expand over `rows` rows of at most `max_cols`
     // columns each and `out_total` counts
@@ -1647,6 +1753,12 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
         TFIM_CUDA(cudaGetLastError());
         k_build_masks<<<sm_count * 8, 256, 0, s>>>(P);
         TFIM_CUDA(cudaGetLastError());
+        if (sup_on) {
+            k_index_mfis<<<sm_count, 256, 0, s>>>(P);
+            k_prune_stack<<<sm_count, 256, 0, s>>>(P);
+            TFIM_CUDA(cudaGetLastError());
+            launches += 2;
+        }
         launches++;
         launches++;
         waves++;
@@ -1695,8 +1807,8 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
             if (hst->jobs == 0) break;   // the stack and the lookahead queue are empty
             TFIM_CHECK(slices < (1LL << 40), TFIM_E_STATE, "resident search did not finish");
         }
-        // per wave: pack, zero, lop3, b1, [proj], expand, masks, control
-        launches += (int64_t)hst->waves * (7 + (with_proj ? 1 : 0));
+        // per wave: pack, zero, lop3, b1, [proj], expand, masks, index, prune, control
+        launches += (int64_t)hst->waves * (9 + (with_proj ? 1 : 0));
         count_launches += (int64_t)hst->waves * (2 + (with_proj ? 1 : 0));
         kernel_ms += (double)hst->count_ns * 1e-6;
     }
@@ -1744,6 +1856,12 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
         TFIM_CUDA(cudaGetLastError());
         k_build_masks<<<sm_count * 8, 256, 0, s>>>(P);
         TFIM_CUDA(cudaGetLastError());
+        if (sup_on) {
+            k_index_mfis<<<sm_count, 256, 0, s>>>(P);
+            k_prune_stack<<<sm_count, 256, 0, s>>>(P);
+            TFIM_CUDA(cudaGetLastError());
+            launches += 2;
+        }
         launches++;
         launches++;
         host_waves++;
@@ -1800,6 +1918,7 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
     stt->lookahead_hits += (int64_t)fin.hits;
     stt->lookaheads_skipped += (int64_t)fin.skipped;
     stt->pruned_pep += (int64_t)fin.pep;
+    stt->pruned_superset += (int64_t)fin.sup_pruned;
     stt->waves += waves;
     stt->launches += launches;
     stt->count_launches += count_launches;

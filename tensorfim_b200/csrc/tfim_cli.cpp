@@ -2,7 +2,7 @@
 //
 //   tfim <transaction file> <minsup fraction> [--engine resident|batched|plain]
 //        [--counter auto|lop3|tensor|i8|proj] [--lookahead 0|1|2|3] [--proposal <file>] [--graphs 0|1]
-//        [--counter auto|lop3|tensor] [--lookahead 0|1]
+//        [--superset 0|1]
 //
 // Same invocation as the reference (code/engine/src/kernel_bitmap.cu:796-798), same
 // result file "<file>-<minsup %f>=Results.txt" next to the input (:906-908), same header
@@ -135,7 +135,7 @@ int main(int argc, char** argv) {
     if (argc < 3) {
         fprintf(stderr, "usage: %s <transaction file> <minsup fraction> [--engine resident|batched|plain] "
                         "[--counter auto|lop3|tensor|i8|proj] [--lookahead 0|1|2|3] [--proposal <weights file>] "
-                        "[--graphs 0|1]\n", argv[0]);
+                        "[--graphs 0|1] [--superset 0|1]\n", argv[0]);
         return 1;
     }
     const char* path = argv[1];
@@ -160,6 +160,7 @@ int main(int argc, char** argv) {
         } else if (k == "--lookahead") opts.lookahead = atoi(v.c_str());
         else if (k == "--proposal") proposal_path = v;
         else if (k == "--graphs") opts.use_graphs = atoi(v.c_str());
+        else if (k == "--superset") opts.superset = atoi(v.c_str());
         else { fprintf(stderr, "unknown option %s\n", k.c_str()); return 1; }
     }
     const double t0 = now();

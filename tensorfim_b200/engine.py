@@ -239,12 +239,15 @@ class Database:
 
     def mine(self, engine: str | None = None, counter: str = "auto", lookahead=True,
              wave_cap: int = 0, top: str = "auto", log_lookahead: bool = False, proj_auto: int = -1,
-             graphs: bool = False, small_pools: bool = False) -> MineResult:
+             graphs: bool = False, small_pools: bool = False, superset: bool = False) -> MineResult:
         """lookahead: False/"off", True/"filtered" (every node passing the exact tail-pair
         filter), "learned" (the attached proposal, or the shipped weights), "all".
         graphs: (resident engine) run the wave loop as a captured CUDA graph whose conditional
         WHILE node repeats pack -> count -> expand on the device; the host reads the status
         only when the search ends or a pool has to grow.
+        superset: (resident engine) drop a family whose head and tail lie inside an MFI already
+        found; the MFI set is the same either way (off by default: it found nothing to drop
+        on the benchmark databases and costs 3-10% of the mine time).
         engine: "resident" (default), "batched" (default for a sharded database) or "plain"."""
         o = _lib.MineOpts()
         lib().tfim_mine_opts_default(C.byref(o))
@@ -260,6 +263,7 @@ class Database:
         o.top_counter = {"auto": 0, "bitmap": 1, "pairs": 2}[top]
         o.use_graphs = int(bool(graphs))
         o.small_pools = int(bool(small_pools))
+        o.superset = int(bool(superset))
         st = _lib.MineStats()
         check(lib().tfim_mine(self._h, C.byref(o), C.byref(st)))
         n = lib().tfim_num_mfis(self._h)
