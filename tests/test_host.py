@@ -62,6 +62,31 @@ def test_cli_usage_and_missing_file(tmp_path):
     assert r.returncode == 1 and "open failed!" in r.stdout
 
 
+@pytest.mark.parametrize("extra,msg", [(["--engine", "fast"], "unknown engine"), (["--counter", "fp8"], "unknown counter"),
+                                       (["--frobnicate", "1"], "unknown option")])
+def test_cli_rejects_unknown_flags_before_reading(tmp_path, extra, msg):
+    r = subprocess.run([_lib.CLI_PATH, str(tmp_path / "nope.txt"), "0.5", *extra], capture_output=True, text=True)
+    assert r.returncode == 1 and msg in r.stderr and "open failed!" not in r.stdout
+
+
+def test_sharded_open_checks_the_group_before_any_device_work():
+    import ctypes as C
+    off = np.array([0, 2], np.int64)
+    items = np.array([1, 2], np.int32)
+    h = C.c_void_p()
+    for rank, world, fn in [(0, 0, None), (2, 2, None), (-1, 2, None), (1, 2, None)]:
+        g = _lib.Group(rank, world, _lib.ALLREDUCE_FN() if fn is None else fn, None)
+        rc = _lib.lib().tfim_open_db_sharded(off.ctypes.data, items.ctypes.data, 1, 0.5, 0, C.byref(g), C.byref(h))
+        assert rc == _lib.TFIM_E_INVALID, (rank, world)
+        assert "tfim_group" in _lib.lib().tfim_last_error().decode()
+        rc = _lib.lib().tfim_open_bitmap_sharded(np.zeros(4, np.uint32).ctypes.data, 1, 64, 1, 0, C.byref(g), C.byref(h))
+        assert rc == _lib.TFIM_E_INVALID
+    assert _lib.lib().tfim_open_db_sharded(off.ctypes.data, items.ctypes.data, 1, 0.5, 0, None, C.byref(h)) \
+        == _lib.TFIM_E_INVALID
+    assert _lib.lib().tfim_mine_all(None, 1, 4, 10, None) == _lib.TFIM_E_INVALID
+    assert _lib.lib().tfim_num_all(None) == -1
+
+
 @pytest.mark.parametrize("name", ["edge_format", "edge_dups", "edge_item0", "edge_single", "cfg1_full"])
 def test_read_fimi_matches_oracle_parse(oracle_mod, tmp_path, name):
     """The Python parser (Database.from_file) follows the reference byte scanner: same row
