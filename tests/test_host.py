@@ -147,3 +147,16 @@ def test_results_parser_and_compare(tmp_path):
     assert tf.load_header(str(p))["MFIsNumber"] == "2"
     c = tf.compare(r, {frozenset({3, 9}): 51})
     assert not c["identical"] and c["freq_mismatch"] == [((3, 9), 50, 51)]
+
+
+def test_levelwise_generator_plants_patterns():
+    from tensorfim_b200.levelwise import generate, support
+    n = 20_000
+    rows, pats = generate(n, 64, 6, seed=1)
+    assert rows.shape == (64, (n + 31) // 32) and rows.dtype == np.uint32
+    assert len(pats) == 6 and all(2 <= len(p) <= 6 and p == sorted(set(p)) for p in pats)
+    bits = np.unpackbits(rows.view(np.uint8), axis=1, bitorder="little")[:, :n].astype(bool)
+    for p in pats:
+        s = support(rows, p)
+        assert s == int(np.logical_and.reduce(bits[p], axis=0).sum())
+        assert s >= int(0.001 * n)   # every pattern fires on at least 0.2% of rows in expectation
