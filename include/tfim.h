@@ -184,19 +184,24 @@ TFIM_API int tfim_count_wave_device(tfim_ctx* ctx, const int32_t* d_item_lists, 
 
 /*
  * Allocation-free form of tfim_count_wave_device, for callers that cannot allocate GPU
- * memory (an allocator that owns the whole device, work recorded while a stream is being
- * captured, code that only holds pointers it was handed).  It needs no context: the
- * caller passes a device bitmap (n_counted rows of words_per_row uint32 words, 16-byte
- * aligned, words_per_row a multiple of 4, bits past the last transaction zero), the
- * device item lists and offsets, and the outputs; the result contract is
- * tfim_count_wave's.  The per-node prefix masks go to a fixed 16 MiB device array
- * inside the library (held on every device that loads it, until exit): a call needing
- * more than b * words_per_row * 4 = 16 MiB is rejected with TFIM_E_INVALID, and so is
- * b > 65535.  The array is shared by all calls and keeps the last call's contents, so
- * calls that overlap on the GPU race.  The first call on a device looks the array's
- * address up (cudaGetSymbolAddress) with that device current; make that first call
- * before any stream capture.  Item ids are not range-checked (they are in device memory).
- * Enqueued on `stream` (NULL = the legacy default stream); returns after enqueueing.
+ * memory: code running inside a memory budget that another allocator owns (it hands out
+ * the whole device up front, so a library cudaMalloc would fail or take memory the
+ * owner has counted on), and code that only holds device pointers it was handed.  It
+ * needs no context: the caller passes a device bitmap, the device item lists and
+ * offsets, and the outputs; the result contract is tfim_count_wave's.
+ *   bitmap: rows of words_per_row uint32 words, 16-byte aligned, words_per_row a multiple
+ *     of 4, bits past the last transaction zero.  Rows 0 .. n_counted-1 are the counted
+ *     items (the columns of counts_out); the bitmap must hold a row for every item id
+ *     that appears in the lists, which may go beyond n_counted.  Item ids are read on the
+ *     device and not range-checked: an id without a row reads outside the bitmap.
+ * The per-node prefix masks go to a fixed 16 MiB device array inside the library (held
+ * on every device that loads it, until exit): a call needing more than
+ * b * words_per_row * 4 = 16 MiB is rejected with TFIM_E_INVALID, and so is b > 65535.
+ * The array is shared by all calls and keeps the last call's contents, so calls that
+ * overlap on the GPU race.  The first call on a device looks the array's address and
+ * the SM count up (cudaGetSymbolAddress, cudaDeviceGetAttribute) with that device
+ * current; make that first call before any stream capture.  Enqueued on `stream`
+ * (NULL = the legacy default stream); returns after enqueueing.
  * No counterpart in the reference.
  */
 TFIM_API int tfim_count_wave_noalloc(const uint32_t* d_bitmap, int64_t words_per_row, int32_t n_counted,

@@ -24,7 +24,8 @@ REF_SERIAL = os.path.join(REF_DIR, "tfim_ref_serial")
 REF_MT = os.path.join(REF_DIR, "tfim_ref_mt")
 REF_GPU = os.path.join(REF_DIR, "tfim_ref_gpu")
 REF_BMMA = os.path.join(REF_DIR, "tfim_ref_bmma")
-REFERENCE_TREE = "/root/reference"
+# the reference project checkout the _ref binaries are compiled from (read in place)
+REFERENCE_TREE = os.environ.get("TFIM_REFERENCE", "/root/reference")
 
 LINE = re.compile(r"^\d+th:\s+\d+\s+\{\s*([^}]*)\}\s+support:\s+\S+\s+frequency:\s+(\d+)")
 

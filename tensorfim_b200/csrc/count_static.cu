@@ -2,8 +2,8 @@
 //
 // Some callers cannot allocate GPU memory at all: code that runs inside a memory
 // budget owned by someone else (an allocator that hands out every byte of a device up
-// front), code that must not add driver allocations while a stream is being captured,
-// and callers that only hold device pointers they were given.  For them this entry
+// front, so a cudaMalloc from a library would fail or steal from it), and callers that
+// only hold device pointers they were given.  For them this entry
 // point does the counting contract of tfim_count_wave_device without a context and
 // without any allocation: the caller passes the bitmap, the item lists and the output
 // buffers, and the per-node prefix masks (the only scratch the count needs) live in a
@@ -29,11 +29,16 @@ __device__ __align__(256) uint32_t g_static_scratch[kTfimStaticScratchBytes / 4]
 
 std::mutex g_static_mu;
 uint32_t* g_static_ptr[64] = {};
+int g_static_sms[64] = {};
 
-int static_scratch(int dev, uint32_t** out) {
+// The scratch array's device address and the SM count of device `dev` (current), looked
+// up once per device.
+int static_scratch(int dev, uint32_t** out, int* sms) {
     TFIM_CHECK(dev >= 0 && dev < 64, TFIM_E_INVALID, "device %d out of range", dev);
     std::lock_guard<std::mutex> lk(g_static_mu);
     if (!g_static_ptr[dev]) {
+        int n_sm = 0;
+        TFIM_CUDA(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
         if (e != cudaSuccess || !p) {
@@ -41,9 +46,11 @@ int static_scratch(int dev, uint32_t** out) {
             set_error("cudaGetSymbolAddress of the static scratch failed on device %d: %s", dev, cudaGetErrorString(e));
             return TFIM_E_CUDA;
         }
+        g_static_sms[dev] = n_sm > 0 ? n_sm : 1;
         g_static_ptr[dev] = static_cast<uint32_t*>(p);
     }
     *out = g_static_ptr[dev];
+    *sms = g_static_sms[dev];
     return TFIM_OK;
 }
 
@@ -132,7 +139,8 @@ extern "C" int tfim_count_wave_noalloc(const uint32_t* d_bitmap, int64_t words_p
     int dev = 0;
     TFIM_CUDA(cudaGetDevice(&dev));
     uint32_t* scratch = nullptr;
-    TFIM_TRY(static_scratch(dev, &scratch));
+    int sms = 1;
+    TFIM_TRY(static_scratch(dev, &scratch, &sms));
     cudaStream_t s = (cudaStream_t)stream;
     const int64_t W = words_per_row;
     if (n_counted > 0) TFIM_CUDA(cudaMemsetAsync(d_counts_out, 0, (size_t)b * n_counted * 4, s));
@@ -144,7 +152,8 @@ extern "C" int tfim_count_wave_noalloc(const uint32_t* d_bitmap, int64_t words_p
     }
     if (n_counted > 0) {
         const int64_t gx = (n_counted + 63) / 64, gy = (b + kStaticRows - 1) / kStaticRows;
-        int64_t slices = std::max<int64_t>(1, (8LL * 148 + gx * gy - 1) / (gx * gy));
+        // about 8 blocks per SM over the word slices
+        int64_t slices = std::max<int64_t>(1, (8LL * sms + gx * gy - 1) / (gx * gy));
         slices = std::min<int64_t>(slices, std::max<int64_t>(1, W / 256));
         const int64_t wslice = ((W / 4 + slices - 1) / slices) * 4;
         const int64_t gz = (W + wslice - 1) / wslice;

@@ -11,9 +11,9 @@ Two groups are provided:
 * ``TorchGroup``: one process per GPU over ``torch.distributed`` (NCCL on NVLink / NVSwitch
   for device buffers).  The all-reduce is enqueued on the library's stream, so the count
   kernels, the collective and the threshold pass stay in stream order without a host sync.
-* ``ThreadGroup``: several shards in one process, one host thread each (on one GPU or
-  several).  The shards meet on the host (a barrier), one thread sums the partial buffers on
-  the GPU, and every shard continues; no kernel waits on another.
+* ``ThreadGroup``: several shards in one process, one host thread each, all on one GPU.
+  The shards meet on the host (a barrier), one thread sums the partial buffers on the GPU,
+  and every shard continues; no kernel waits on another.
 
 Every shard must make the same library calls in the same order (the collectives match by
 order); a shard that fails leaves the others to the group's timeout, after which their call
@@ -110,9 +110,10 @@ class TorchGroup(Group):
 
 
 class ThreadGroup:
-    """`world` shards in one process, one host thread each.
+    """`world` shards in one process, one host thread each, all on one GPU (`device`).
 
-    ``run(fn)`` calls ``fn(member)`` in one thread per shard and returns the results in rank
+    Every shard's context must be opened on `device`: the reduction views every shard's
+    buffer as memory of that device.  ``run(fn)`` calls ``fn(member)`` in one thread per shard and returns the results in rank
     order; ``member.allreduce`` waits (on the host, up to `timeout` seconds) for every shard's
     partial buffer, sums them on the GPU into every buffer, and returns."""
 

@@ -10,7 +10,8 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
-REFERENCE = "/root/reference"   # present only where the reference tree is mounted
+# the reference project checkout, present only where it is mounted
+REFERENCE = os.environ.get("TFIM_REFERENCE", "/root/reference")
 
 
 def pytest_configure(config):

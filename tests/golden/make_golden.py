@@ -13,7 +13,8 @@ runs it on
 Each fixture <name>.json.gz holds the spec, the reference's header statistics and its MFIs
 as [sorted item list, frequency] pairs.
 
-Run from the repository root:  python tests/golden/make_golden.py
+Run from the repository root:  python tests/golden/make_golden.py [name ...]
+(with names, only those fixtures are regenerated).
 """
 from __future__ import annotations
 
@@ -40,6 +41,10 @@ SYNTH = [
     ("cfg5_s002", 5, {"scale": 0.02}, 0.70),
     ("cfg5_s002_t40", 5, {"scale": 0.02}, 0.40),
     ("cfg1_t03", 1, {"scale": 0.5}, 0.03),
+    # the replicated 12.54M configuration's generator at its base size (1 replica) with the
+    # minimum support lowered from 85% to 6% (at 85% no item is frequent); supports of the
+    # 256-replica database are exactly 256x these
+    ("cfg3_base_t06", 3, {"replicas": 1}, 0.06),
 ]
 
 
@@ -88,11 +93,13 @@ def edge_files() -> dict:
     return out
 
 
-def main() -> None:
+def main(only: list[str]) -> None:
     if not os.path.exists(oracle.REF_SERIAL):
         oracle.build()
     with tempfile.TemporaryDirectory() as d:
         for name, cfg, kw, minsup in SYNTH:
+            if only and name not in only:
+                continue
             db = synth.generate(cfg, **kw)
             path = os.path.join(d, name + ".txt")
             synth.write_fimi(path, db)
@@ -100,6 +107,8 @@ def main() -> None:
             spec = {"kind": "synth", "config": cfg, "kwargs": kw, "minsup": minsup}
             _dump(name, spec, hdr, mfis)
         for name, (blob, minsup) in edge_files().items():
+            if only and name not in only:
+                continue
             path = os.path.join(HERE, name + ".txt")
             with open(path, "wb") as f:
                 f.write(blob)
@@ -124,4 +133,4 @@ def _dump(name, spec, hdr, mfis):
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

@@ -1,13 +1,15 @@
 """tfim_count_wave_noalloc: counting with no GPU allocation, checked against
-tfim_count_wave_device on the same inputs, twice in a row.
+tfim_count_wave_device and against the oracle's counter on the same inputs, twice in a
+row, with the device memory in use unchanged across a call.
 
-The allocation-free entry point serves callers that cannot call cudaMalloc (a memory
-budget owned by another allocator, work recorded during stream capture, code that only
-holds device pointers it was handed).  Its scratch is a fixed device array inside the
-library that every call shares, so two consecutive calls must both be exact: the second
-must not see anything left over from the first.  Counts are integers, so the tolerance is
-zero.  This file is collected last so that a failure here stops a -x run only after
-every other test has run; it passes alone and after the rest."""
+The allocation-free entry point serves callers that cannot call cudaMalloc: code inside a
+memory budget that another allocator owns, and code that only holds device pointers it
+was handed.  Its scratch is a fixed device array inside the library that every call
+shares, so two consecutive calls must both be exact: the second must not see anything
+left over from the first.  Counts are integers, so the tolerance is zero.  The item lists
+name rows beyond the counted ones (the bitmap holds 90 rows, 70 are counted).  This file
+is collected last so that a failure here stops a -x run only after every other test has
+run; it passes alone and after the rest."""
 import ctypes as C
 
 import numpy as np
@@ -38,7 +40,13 @@ def _wave(b, n_rows, seed):
     return lists, offs, flat
 
 
-def test_noalloc_matches_count_wave_device_on_two_calls():
+def _noalloc(t_bitmap, W, d, t_items, t_offs, b, min_count, got_c, got_n, stream):
+    return _lib.lib().tfim_count_wave_noalloc(C.c_void_p(t_bitmap.data_ptr()), W, d, C.c_void_p(t_items.data_ptr()),
+                                              C.c_void_p(t_offs.data_ptr()), b, min_count, C.c_void_p(got_c.data_ptr()),
+                                              C.c_void_p(got_n.data_ptr()), C.c_void_p(stream))
+
+
+def test_noalloc_matches_count_wave_device_on_two_calls(oracle_mod):
     import torch
     n_rows, d, n_bits = 90, 70, 150_001
     rows = _rows(n_rows, n_bits, seed=21)
@@ -52,6 +60,7 @@ def test_noalloc_matches_count_wave_device_on_two_calls():
     with tf.Database.from_bitmap(rows, n_bits, d) as db:
         for call, (b, seed) in enumerate([(53, 5), (37, 6)]):
             lists, offs, flat = _wave(b, n_rows, seed)
+            assert max(flat) >= d, "the lists must name rows beyond the counted ones"
             min_count = 4000
             t_items = torch.from_numpy(flat).to(dev)
             t_offs = torch.from_numpy(offs).to(dev)
@@ -61,14 +70,20 @@ def test_noalloc_matches_count_wave_device_on_two_calls():
                                  ref_n.data_ptr(), stream)
             got_c = torch.full((b, d), -7, dtype=torch.int32, device=dev)
             got_n = torch.full((b,), -7, dtype=torch.int32, device=dev)
-            rc = _lib.lib().tfim_count_wave_noalloc(C.c_void_p(t_bitmap.data_ptr()), W, d, C.c_void_p(t_items.data_ptr()),
-                                                    C.c_void_p(t_offs.data_ptr()), b, min_count,
-                                                    C.c_void_p(got_c.data_ptr()), C.c_void_p(got_n.data_ptr()),
-                                                    C.c_void_p(stream))
-            _lib.check(rc)
             torch.cuda.synchronize()
-            assert torch.equal(got_c, ref_c), f"call {call}: counts differ"
-            assert torch.equal(got_n, ref_n), f"call {call}: nfreq differ"
+            free0, _ = torch.cuda.mem_get_info(dev)
+            alloc0 = torch.cuda.memory_allocated(dev)
+            _lib.check(_noalloc(t_bitmap, W, d, t_items, t_offs, b, min_count, got_c, got_n, stream))
+            torch.cuda.synchronize()
+            free1, _ = torch.cuda.mem_get_info(dev)
+            if call > 0:   # the first call on a device may load the library's module
+                assert free1 == free0, f"call {call}: device free memory changed by {free0 - free1} bytes"
+            assert torch.cuda.memory_allocated(dev) == alloc0
+            assert torch.equal(got_c, ref_c), f"call {call}: counts differ from tfim_count_wave_device"
+            assert torch.equal(got_n, ref_n), f"call {call}: nfreq differ from tfim_count_wave_device"
+            exp_c, exp_n = oracle_mod.count_wave(rows, lists, d, min_count)
+            assert np.array_equal(got_c.cpu().numpy(), exp_c), f"call {call}: counts differ from the oracle"
+            assert np.array_equal(got_n.cpu().numpy(), exp_n), f"call {call}: nfreq differ from the oracle"
 
 
 def test_noalloc_rejects_a_wave_beyond_the_scratch():
