@@ -259,7 +259,34 @@ typedef struct {
     int64_t lookaheads_skipped;/* lookaheads ruled out because a tail pair is infrequent */
     double  top_ms;            /* CUDA-event time of counting the empty-prefix family (resident) */
     int64_t pruned_superset;   /* families dropped by the superset check (resident) */
+    /* per counting path (index TFIM_PATH_*): device time of its launches, algorithmic bytes
+       (every operand row read once as a dense row, every count written once), bit-ops
+       (supports x transactions), supports and launches.  Device times come from CUDA events
+       around the host-driven launches and from %globaltimer stamps at the start of each
+       kernel of a wave (the time from one phase's start to the next phase's start). */
+    double  path_ms[6];
+    int64_t path_bytes[6];
+    int64_t path_bitops[6];
+    int64_t path_supports[6];
+    int64_t path_launches[6];
+    /* device time of the other phases of the search (same stamps): wave packing, row
+       expansion, prefix-mask building, and the count-block zeroing */
+    double  pack_ms;
+    double  expand_ms;
+    double  mask_ms;
+    double  zero_ms;
+    /* host time before the first search launch (pool growth, initial state) and after the
+       last one (MFI read-back and assembly, result ordering) */
+    double  setup_ms;
+    double  readback_ms;
 } tfim_mine_stats;
+
+/* counting paths of tfim_mine_stats.path_* */
+#define TFIM_PATH_LOP3   0   /* AND + popc tiles on CUDA cores */
+#define TFIM_PATH_B1     1   /* b1 AND+POPC mma.sync tiles */
+#define TFIM_PATH_TC     2   /* tcgen05.mma kind::i8 tiles (bits expanded to bytes) */
+#define TFIM_PATH_PAIRS  3   /* pair co-occurrence over the reduced transaction list */
+#define TFIM_PATH_PROJ   4   /* projected counting over the prefix's transactions */
 
 /* ------------------------------------------------------------------ tuning table
  * Launch shapes and counter selection of the engines.  The reference fixes these as

@@ -185,20 +185,30 @@ def load_results(path: str) -> dict:
 
 
 def run_reference(path: str, minsup: float, binary: str = REF_SERIAL, threads: int | None = None,
-                  timeout: float = 600) -> tuple[dict, dict]:
+                  timeout: float = 600, in_place: bool = False, stdout: dict | None = None) -> tuple[dict, dict]:
     """Run a reference binary on a copy of `path` in a scratch directory (its results file
-    is written next to its input).  Returns (mfis, header)."""
+    is written next to its input), or on `path` itself with `in_place` (its directory must
+    be writable; the results file is removed afterwards).  Returns (mfis, header); when
+    `stdout` is a dict, its "text" gets the run's standard output and "wall_s" its wall time."""
     if not os.path.exists(binary):
         raise FileNotFoundError(binary)
     with tempfile.TemporaryDirectory() as d:
-        dst = os.path.join(d, os.path.basename(path))
-        shutil.copyfile(path, dst)
+        if in_place:
+            dst = path
+        else:
+            dst = os.path.join(d, os.path.basename(path))
+            shutil.copyfile(path, dst)
         env = dict(os.environ)
         if threads:
             env["TFIM_REF_THREADS"] = str(threads)
             env["OMP_NUM_THREADS"] = str(threads)
+        import time
+        t0 = time.perf_counter()
         r = subprocess.run([binary, dst, "%r" % float(minsup)], capture_output=True, text=True, env=env,
-                           timeout=timeout, cwd=d)
+                           timeout=timeout, cwd=os.path.dirname(os.path.abspath(dst)))
+        if stdout is not None:
+            stdout["text"] = r.stdout
+            stdout["wall_s"] = time.perf_counter() - t0
         res = "%s-%f=Results.txt" % (dst, minsup)
         if not os.path.exists(res):
             raise RuntimeError(f"reference run produced no results file (rc={r.returncode}): {r.stdout[-500:]} {r.stderr[-500:]}")
@@ -208,4 +218,7 @@ def run_reference(path: str, minsup: float, binary: str = REF_SERIAL, threads: i
                 m = re.match(r"^([A-Za-z_()]+):\s*(\S+)", ln.strip())
                 if m and m.group(1) not in header:
                     header[m.group(1)] = m.group(2)
-        return load_results(res), header
+        mfis = load_results(res)
+        if in_place:
+            os.unlink(res)
+        return mfis, header

@@ -103,10 +103,22 @@ class MineStats(C.Structure):
                 ("waves", C.c_int64), ("launches", C.c_int64), ("count_launches", C.c_int64),
                 ("lookaheads", C.c_int64), ("lookahead_hits", C.c_int64), ("pruned_pep", C.c_int64),
                 ("n_mfi", C.c_int64), ("host_ms", C.c_double), ("sync_ms", C.c_double),
-                ("lookaheads_skipped", C.c_int64), ("top_ms", C.c_double), ("pruned_superset", C.c_int64)]
+                ("lookaheads_skipped", C.c_int64), ("top_ms", C.c_double), ("pruned_superset", C.c_int64),
+                ("path_ms", C.c_double * 6), ("path_bytes", C.c_int64 * 6), ("path_bitops", C.c_int64 * 6),
+                ("path_supports", C.c_int64 * 6), ("path_launches", C.c_int64 * 6),
+                ("pack_ms", C.c_double), ("expand_ms", C.c_double), ("mask_ms", C.c_double), ("zero_ms", C.c_double),
+                ("setup_ms", C.c_double), ("readback_ms", C.c_double)]
 
     def as_dict(self) -> dict:
-        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+        out = {}
+        for k, _ in self._fields_:
+            v = getattr(self, k)
+            out[k] = list(v) if k.startswith("path_") else v
+        return out
+
+
+# counting paths of MineStats.path_* (include/tfim.h TFIM_PATH_*)
+PATHS = ["lop3", "b1", "tc", "pairs", "proj"]
 
 
 _lib = None

@@ -409,6 +409,11 @@ int tfim_mine(tfim_ctx* c, const tfim_mine_opts* opts, tfim_mine_stats* stats) {
         c->mfis.sup.swap(S.sup);
     }
     st.n_mfi = (int64_t)c->mfis.size();
+    // computation time as the reference reports it: search and counting, bitmap resident,
+    // results in host memory in their output order
+    const auto t2 = std::chrono::steady_clock::now();
+    st.mine_seconds = std::chrono::duration<double>(t2 - t0).count();
+    st.readback_ms += std::chrono::duration<double, std::milli>(t2 - t1).count();
     c->mined = true;
     c->last_stats = st;
     if (stats) *stats = st;

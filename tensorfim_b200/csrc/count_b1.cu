@@ -210,7 +210,9 @@ __device__ void b1_tile(const CountArgs& a, const TileDesc t, unsigned char* sme
 __global__ void __launch_bounds__(256) k_count_b1(CountArgs a) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ B1Shared sh;
+    phase_begin(a.ph_s);
     b1_tile(a, a.tiles[blockIdx.x], smem, sh);
+    phase_end(a.ph_e);
 }
 
 __global__ void __launch_bounds__(256) k_count_b1_persistent(const CountArgs* __restrict__ args, const int32_t* n_tiles,
@@ -220,6 +222,7 @@ __global__ void __launch_bounds__(256) k_count_b1_persistent(const CountArgs* __
     __shared__ int32_t s_t;
     const CountArgs a = *args;
     const int32_t n = *n_tiles;
+    phase_begin(a.ph_s);
     while (true) {
         if (threadIdx.x == 0) s_t = atomicAdd(next, 1);
         __syncthreads();
@@ -228,6 +231,7 @@ __global__ void __launch_bounds__(256) k_count_b1_persistent(const CountArgs* __
         if (t >= n) break;
         b1_tile(a, a.tiles[t], smem, sh);
     }
+    phase_end(a.ph_e);
 }
 
 }  // namespace

@@ -185,7 +185,9 @@ __device__ __forceinline__ void lop3_tile(const CountArgs& a, const TileDesc t, 
 
 __global__ void __launch_bounds__(256, 4) k_count_lop3(CountArgs a) {
     __shared__ Lop3Shared sh;
+    phase_begin(a.ph_s);
     lop3_tile(a, a.tiles[blockIdx.x], sh);
+    phase_end(a.ph_e);
 }
 
 // Persistent form: arguments and tile count are read from device memory (a wave built on the
@@ -197,6 +199,7 @@ __global__ void __launch_bounds__(256, 4) k_count_lop3_persistent(const CountArg
     __shared__ int32_t s_t;
     const CountArgs a = *args;
     const int32_t n = *n_tiles;
+    phase_begin(a.ph_s);
     while (true) {
         if (threadIdx.x == 0) s_t = atomicAdd(next, 1);
         __syncthreads();
@@ -205,6 +208,7 @@ __global__ void __launch_bounds__(256, 4) k_count_lop3_persistent(const CountArg
         if (t >= n) break;
         lop3_tile(a, a.tiles[t], sh);
     }
+    phase_end(a.ph_e);
 }
 
 // masks[dst] = (src >= 0 ? masks[src] : ~0) & AND of the listed item rows.

@@ -173,7 +173,9 @@ __global__ void __launch_bounds__(kProjWarps * 32) k_count_proj(CountArgs a, con
                                                                 const int64_t* __restrict__ red_off,
                                                                 const int32_t* __restrict__ red_items) {
     __shared__ ProjShared sh;
+    phase_begin(a.ph_s);
     proj_job(a, job_ids[blockIdx.x], red_off, red_items, sh);
+    phase_end(a.ph_e);
 }
 
 __global__ void __launch_bounds__(kProjWarps * 32) k_count_proj_persistent(const CountArgs* __restrict__ args,
@@ -183,7 +185,9 @@ __global__ void __launch_bounds__(kProjWarps * 32) k_count_proj_persistent(const
     __shared__ ProjShared sh;
     const CountArgs a = *args;
     const int32_t n = *n_jobs;
+    phase_begin(a.ph_s);
     for (int32_t q = blockIdx.x; q < n; q += gridDim.x) proj_job(a, a.job_list[q], red_off, red_items, sh);
+    phase_end(a.ph_e);
 }
 
 }  // namespace

@@ -180,6 +180,10 @@ struct WaveRunner {
     double sync_ms = 0;
     int32_t counter = TFIM_COUNTER_AUTO;
     int sm_count = 148;
+    // per counting path (TFIM_PATH_*): device time, algorithmic bytes, bit-ops, supports, launches
+    double path_ms[6] = {};
+    int64_t path_bytes[6] = {}, path_bitops[6] = {}, path_supports[6] = {}, path_launches[6] = {};
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};   // before pairs, lop3, b1; after b1
 
     void reset_counters() {
         launches = 0;
@@ -187,6 +191,27 @@ struct WaveRunner {
         bytes_alg = 0;
         kernel_ms = 0;
         sync_ms = 0;
+        for (int q = 0; q < 6; q++) {
+            path_ms[q] = 0;
+            path_bytes[q] = path_bitops[q] = path_supports[q] = path_launches[q] = 0;
+        }
+    }
+    void add_to(tfim_mine_stats* st) const {
+        for (int q = 0; q < 6; q++) {
+            st->path_ms[q] += path_ms[q];
+            st->path_bytes[q] += path_bytes[q];
+            st->path_bitops[q] += path_bitops[q];
+            st->path_supports[q] += path_supports[q];
+            st->path_launches[q] += path_launches[q];
+        }
+    }
+    // device time of the wave's counting launches per path (the events of this wave are done)
+    void read_path_times(bool pairs, bool l3, bool b1) {
+        float ms = 0;
+        if (pairs && cudaEventElapsedTime(&ms, ev[0], ev[1]) == cudaSuccess) path_ms[TFIM_PATH_PAIRS] += ms;
+        if (l3 && cudaEventElapsedTime(&ms, ev[1], ev[2]) == cudaSuccess) path_ms[TFIM_PATH_LOP3] += ms;
+        if (b1 && cudaEventElapsedTime(&ms, ev[2], ev[3]) == cudaSuccess) path_ms[TFIM_PATH_B1] += ms;
+        if (cudaEventElapsedTime(&ms, ev[0], ev[3]) == cudaSuccess) kernel_ms += ms;
     }
 
     int run(Wave& w, int32_t min_count, bool want_full_counts, std::vector<int32_t>* full_counts) {
@@ -220,13 +245,22 @@ struct WaveRunner {
         const int64_t row_bytes = (c->n_bits + 7) / 8;
         for (size_t j = 0; j < w.jobs.size(); j++) {
             const JobDesc& jd = w.jobs[j];
+            const int64_t sup = (int64_t)jd.n_rows * jd.n_cols;
             if ((int32_t)j == w.top_job && w.top_mode == 2) {
                 // pair counting reads the reduced transaction list and writes the matrix
-                bytes_alg += (c->d_red_off ? (c->n_bits + 1) * 8 + c->n_red_items * 4 : 0) + 4LL * jd.n_rows * jd.n_cols;
+                const int64_t by = (c->d_red_off ? (c->n_bits + 1) * 8 + c->n_red_items * 4 : 0) + 4LL * sup;
+                bytes_alg += by;
+                path_bytes[TFIM_PATH_PAIRS] += by;
+                path_supports[TFIM_PATH_PAIRS] += sup;
                 continue;
             }
             const int64_t base_rows = (jd.base_slot >= 0) + (jd.base_item >= 0);
-            bytes_alg += row_bytes * (jd.n_rows + jd.n_cols + base_rows) + 4LL * jd.n_rows * jd.n_cols;
+            const int64_t by = row_bytes * (jd.n_rows + jd.n_cols + base_rows) + 4LL * sup;
+            const int q = w.use_b1[j] ? TFIM_PATH_B1 : TFIM_PATH_LOP3;
+            bytes_alg += by;
+            path_bytes[q] += by;
+            path_bitops[q] += sup * c->n_bits;
+            path_supports[q] += sup;
         }
         for (size_t j = 0; j < w.jobs.size(); j++) {
             const bool top = (int32_t)j == w.top_job;
@@ -271,27 +305,35 @@ struct WaveRunner {
         a.bitmap = c->d_bitmap; a.W = W; a.masks = c->d_masks.as<uint32_t>();
         a.jobs = (const JobDesc*)(db + o_jobs); a.rows = (const RowDesc*)(db + o_rows);
         a.cols = (const int32_t*)(db + o_cols); a.out = d_counts.as<int32_t>();
-        TFIM_CUDA(cudaEventRecord(c->ev0, s));
-        if (w.top_job >= 0 && w.top_mode == 2) {
+        for (int q = 0; q < 4; q++)
+            if (!ev[q]) TFIM_CUDA(cudaEventCreate(&ev[q]));
+        const bool run_pairs = w.top_job >= 0 && w.top_mode == 2;
+        TFIM_CUDA(cudaEventRecord(ev[0], s));
+        if (run_pairs) {
             const JobDesc& tj = w.jobs[w.top_job];
             TFIM_TRY(launch_pair_count(c->d_red_off, c->d_red_items, c->n_bits, (const int32_t*)(db + o_tpos), tj.n_rows,
                                        d_counts.as<int32_t>() + tj.out_off, s));
             launches++;
             count_launches++;
+            path_launches[TFIM_PATH_PAIRS]++;
         }
+        TFIM_CUDA(cudaEventRecord(ev[1], s));
         if (!t_l3.empty()) {
             a.tiles = (const TileDesc*)(db + o_tl3); a.n_tiles = (int32_t)t_l3.size();
             TFIM_TRY(launch_count_lop3(a, s));
             launches++;
             count_launches++;
+            path_launches[TFIM_PATH_LOP3]++;
         }
+        TFIM_CUDA(cudaEventRecord(ev[2], s));
         if (!t_b1.empty()) {
             a.tiles = (const TileDesc*)(db + o_tb1); a.n_tiles = (int32_t)t_b1.size();
             TFIM_TRY(launch_count_b1(a, s));
             launches++;
             count_launches++;
+            path_launches[TFIM_PATH_B1]++;
         }
-        TFIM_CUDA(cudaEventRecord(c->ev1, s));
+        TFIM_CUDA(cudaEventRecord(ev[3], s));
         // a transaction-sharded context sums the partial counts of the whole wave over the group
         TFIM_TRY(group_reduce(c, d_counts.p, w.out_total, TFIM_DT_I32, TFIM_RED_SUM, s));
         if (w.top_job >= 0) {
@@ -306,9 +348,7 @@ struct WaveRunner {
             const double ts0 = now_s();
             TFIM_CUDA(cudaStreamSynchronize(s));
             sync_ms += (now_s() - ts0) * 1e3;
-            float ms = 0;
-            cudaEventElapsedTime(&ms, c->ev0, c->ev1);
-            kernel_ms += ms;
+            read_path_times(run_pairs, !t_l3.empty(), !t_b1.empty());
             return TFIM_OK;
         }
         // compact: entries >= min_count per row
@@ -324,9 +364,7 @@ struct WaveRunner {
         const double ts0 = now_s();
         TFIM_CUDA(cudaStreamSynchronize(s));
         sync_ms += (now_s() - ts0) * 1e3;
-        float ms = 0;
-        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
-        kernel_ms += ms;
+        read_path_times(run_pairs, !t_l3.empty(), !t_b1.empty());
         const int2* ri = h_rowinfo.as<int2>();
         const int32_t total = *(const int32_t*)(ri + n_rows);
         row_info.assign(ri, ri + n_rows);
@@ -344,6 +382,11 @@ struct WaveRunner {
     void release() {
         d_desc.release(); d_counts.release(); d_entries.release(); d_rowinfo.release();
         h_desc.release(); h_rowinfo.release(); h_entries.release();
+        for (cudaEvent_t& e : ev)
+            if (e) {
+                cudaEventDestroy(e);
+                e = nullptr;
+            }
     }
 };
 
@@ -493,6 +536,7 @@ int mine_plain(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* st) {
     st->bytes_alg += wr.bytes_alg;
     st->kernel_ms += wr.kernel_ms;
     st->sync_ms += wr.sync_ms;
+    wr.add_to(st);
     return rc;
 }
 
@@ -506,6 +550,7 @@ int mine_plain_roots(tfim_ctx* c, const std::vector<int32_t>& roots, tfim_mine_s
     st->bytes_alg += wr.bytes_alg;
     st->kernel_ms += wr.kernel_ms;
     st->sync_ms += wr.sync_ms;
+    wr.add_to(st);
     return rc;
 }
 
@@ -862,6 +907,7 @@ int mine_batched(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* st) {
     st->bytes_alg += wr.bytes_alg;
     st->kernel_ms += wr.kernel_ms;
     st->sync_ms += wr.sync_ms;
+    wr.add_to(st);
     st->bit_ops = st->supports * c->n_bits;
     (void)W;
     return TFIM_OK;

@@ -58,6 +58,10 @@ struct DJob {
                                // jobs' (prefix b3l after all heavy tiles)
 };
 
+// Phases of a wave (device-time stamps) and counter classes of a count job.
+enum { kPhPack = 0, kPhZero, kPhLop3, kPhB1, kPhTc, kPhProj, kPhExpand, kPhMasks, kPhases };
+enum { kClsLop3 = 0, kClsB1 = 1, kClsProj = 2, kClsTc = 3, kClasses = 4 };
+
 struct ResStatus {
     int32_t stack_n, look_n, fam_n, item_n, head_n, mfi_n, mfi_item_n, slot_n, free_n, free_taken, defer_n, log_n;
     int32_t jobs, rows, tiles_l3, tiles_b1, n_proj, n_mjobs;   // n_mjobs: masks the last expand asked for
@@ -68,11 +72,17 @@ struct ResStatus {
     int32_t grow, g_rows, g_jobs, g_max_head, g_max_cols, waves;
     int64_t g_out, g_tiles;
     int32_t launch_id, next3, next1, pad1;   // next3 / next1: tile counters of the persistent counters
-    unsigned long long launch_t0, count_t0;
-    unsigned long long supports, nodes, lookaheads, hits, skipped, pep, bytes_alg, count_ns;
+    unsigned long long launch_t0;
+    unsigned long long supports, nodes, lookaheads, hits, skipped, pep;
     // superset check: MFIs [0, sup_done) are in the item -> MFI index the expand reads
     int32_t sup_done, pad2;
     unsigned long long sup_pruned;
+    // phase stamps of the current wave (first block start, last block end; %globaltimer ns)
+    // and their durations summed over the search; the pack folds and resets them
+    unsigned long long ph_s[kPhases], ph_e[kPhases], ph_ns[kPhases];
+    // committed count jobs per counter class: algorithmic bytes (every operand row read once,
+    // every count written once), bit-ops (supports x transactions), supports, jobs
+    unsigned long long cls_bytes[kClasses], cls_bitops[kClasses], cls_sup[kClasses], cls_jobs[kClasses];
 };
 
 // Pool capacities, in entries.  A wave is packed only when the worst case of its expand fits.
@@ -164,14 +174,10 @@ __host__ __device__ __forceinline__ int column_block(int nF) { return max(128, (
 // only rewrites this record (the captured launches stay valid).
 struct ResArgs {
     ResPtrs p;
-    CountArgs a3, a1;
+    CountArgs a3, a1, ap;   // CUDA-core, b1 and projected counters
 };
 
-__device__ __forceinline__ unsigned long long globaltimer() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
+__device__ __forceinline__ unsigned long long globaltimer() { return dev_globaltimer(); }
 
 // Projected counting pays when the prefix holds few transactions: it walks the base's set
 // bits (W words) and looks up about 6 entries per item of each of its sup transactions,
@@ -258,6 +264,14 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
             st->launch_id = p.launch_id;
             st->launch_t0 = globaltimer();
         }
+        // the last wave's phases: add their durations, clear the stamps, stamp this pack
+        for (int k = 0; k < kPhases; k++) {
+            const unsigned long long s0 = st->ph_s[k], e0 = st->ph_e[k];
+            if (s0 != ~0ull && e0 > s0) st->ph_ns[k] += e0 - s0;
+            st->ph_s[k] = ~0ull;
+            st->ph_e[k] = 0;
+        }
+        st->ph_s[kPhPack] = globaltimer();
     }
     __syncthreads();
     if (tid == 0) {
@@ -562,6 +576,7 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
     if (!s_fit) {
         if (tid == 0) {
             st->jobs = 0; st->rows = 0; st->tiles_l3 = 0; st->tiles_b1 = 0; st->n_proj = 0; st->out_total = 0;
+            st->ph_e[kPhPack] = globaltimer();
         }
         return;
     }
@@ -569,6 +584,44 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
     for (int j = n_look + tid; j < nj; j += kPackThreads) {
         const DJob dj = p.djobs[j];
         p.fams[dj.fam].next_row = dj.r0 + dj.nr;
+    }
+    // the wave's work per counter class (warp sums, one atomic per warp and class)
+    {
+        unsigned long long cb[kClasses], cbo[kClasses], cs[kClasses], cj[kClasses];
+#pragma unroll
+        for (int k = 0; k < kClasses; k++) cb[k] = cbo[k] = cs[k] = cj[k] = 0;
+        for (int j = tid; j < nj; j += kPackThreads) {
+            const JobDesc jd = p.jobs[j];
+            const int cls = p.djobs[j].cls;
+            const unsigned long long nbase = (jd.base_slot >= 0) + (jd.base_item >= 0);
+            const unsigned long long sup = (unsigned long long)jd.n_rows * (unsigned long long)jd.n_cols;
+            const unsigned long long by =
+                (unsigned long long)p.row_bytes * ((unsigned long long)jd.n_rows + jd.n_cols + nbase) + 4ull * sup;
+#pragma unroll
+            for (int k = 0; k < kClasses; k++)
+                if (cls == k) {
+                    cb[k] += by;
+                    cbo[k] += sup * (unsigned long long)p.n_bits;
+                    cs[k] += sup;
+                    cj[k] += 1;
+                }
+        }
+#pragma unroll
+        for (int k = 0; k < kClasses; k++) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                cb[k] += __shfl_xor_sync(0xffffffffu, cb[k], o);
+                cbo[k] += __shfl_xor_sync(0xffffffffu, cbo[k], o);
+                cs[k] += __shfl_xor_sync(0xffffffffu, cs[k], o);
+                cj[k] += __shfl_xor_sync(0xffffffffu, cj[k], o);
+            }
+            if ((tid & 31) == 0 && cj[k]) {
+                atomicAdd(&st->cls_bytes[k], cb[k]);
+                atomicAdd(&st->cls_bitops[k], cbo[k]);
+                atomicAdd(&st->cls_sup[k], cs[k]);
+                atomicAdd(&st->cls_jobs[k], cj[k]);
+            }
+        }
     }
     if (T3 <= p.cap_tiles)
         for (int64_t t = tid; t < T3; t += kPackThreads) {
@@ -610,7 +663,7 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
         st->look_n = 0;
         st->nodes += rows_total;
         st->supports += s_out_total;
-        st->bytes_alg += (unsigned long long)(p.row_bytes * (2LL * rows_total + nj) + 4 * s_out_total);
+        st->ph_e[kPhPack] = globaltimer();
     }
 }
 
@@ -1097,9 +1150,10 @@ __device__ void expand_row(const ResPtrs& p, int64_t g, int lane) {
 }
 
 __global__ void __launch_bounds__(256) k_res_expand(ResPtrs p) {
+    phase_begin(&p.st->ph_s[kPhExpand]);
     const int64_t g = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    if (g >= p.st->rows) return;
-    expand_row(p, g, threadIdx.x & 31);
+    if (g < p.st->rows) expand_row(p, g, threadIdx.x & 31);
+    phase_end(&p.st->ph_e[kPhExpand]);
 }
 
 // The masks the expand asked for, with the whole grid: units of 1,024 128-bit words of one
@@ -1129,7 +1183,11 @@ __device__ __forceinline__ void build_masks(const ResPtrs& p) {
         }
     }
 }
-__global__ void __launch_bounds__(256) k_build_masks(ResPtrs p) { build_masks(p); }
+__global__ void __launch_bounds__(256) k_build_masks(ResPtrs p) {
+    phase_begin(&p.st->ph_s[kPhMasks]);
+    build_masks(p);
+    phase_end(&p.st->ph_e[kPhMasks]);
+}
 
 // Add the MFIs emitted since the last pack to the superset index: one warp per MFI, one
 // atomicOr per item.  An MFI holding an item beyond the index is left out (it then prunes
@@ -1153,7 +1211,11 @@ __device__ void index_mfis(const ResPtrs& p) {
             atomicOr(&p.sup_index[(int64_t)p.mfi_items[off + q] * p.sup_words + (k >> 5)], bit);
     }
 }
-__global__ void __launch_bounds__(256) k_index_mfis(ResPtrs p) { index_mfis(p); }
+__global__ void __launch_bounds__(256) k_index_mfis(ResPtrs p) {
+    phase_begin(&p.st->ph_s[kPhMasks]);
+    index_mfis(p);
+    phase_end(&p.st->ph_e[kPhMasks]);
+}
 
 // Families waiting on the stack that an MFI found since their creation covers: a fresh
 // family (no row handed out, not waiting on a lookahead) whose head and whole tail lie inside
@@ -1179,7 +1241,11 @@ __device__ void prune_stack(const ResPtrs& p) {
         }
     }
 }
-__global__ void __launch_bounds__(256) k_prune_stack(ResPtrs p) { prune_stack(p); }
+__global__ void __launch_bounds__(256) k_prune_stack(ResPtrs p) {
+    phase_begin(&p.st->ph_s[kPhMasks]);
+    prune_stack(p);
+    phase_end(&p.st->ph_e[kPhMasks]);
+}
 
 // The expand's first pass for the family of the empty prefix (an n x n count block whose
 // rows are its tail, nT = nF = n): one block per row streams the row with four loads in
@@ -1237,12 +1303,12 @@ __global__ void __launch_bounds__(256) k_top_summary(const int32_t* __restrict__
 // is done, when the pack asks for larger pools or reports an error, or after the slice's
 // wave / time limit; the host then reads the status once.
 
-// Zero the wave's count block; stamps the start of counting.
+// Zero the wave's count block and the persistent counters' tile counters.
 __global__ void __launch_bounds__(256) k_res_zero(const ResArgs* __restrict__ args) {
     ResStatus* st = args->p.st;
     int32_t* counts = args->p.counts;
+    phase_begin(&st->ph_s[kPhZero]);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-        st->count_t0 = globaltimer();
         st->next3 = 0;
         st->next1 = 0;
     }
@@ -1253,24 +1319,36 @@ __global__ void __launch_bounds__(256) k_res_zero(const ResArgs* __restrict__ ar
     int4* c4 = reinterpret_cast<int4*>(counts);
     for (int64_t i = i0; i < n4; i += stride) c4[i] = make_int4(0, 0, 0, 0);
     for (int64_t i = (n4 << 2) + i0; i < n; i += stride) counts[i] = 0;
+    phase_end(&st->ph_e[kPhZero]);
 }
 
 __global__ void __launch_bounds__(256) k_res_expand_g(const ResArgs* __restrict__ args) {
     const ResPtrs p = args->p;
     const int lane = threadIdx.x & 31;
+    phase_begin(&p.st->ph_s[kPhExpand]);
     const int32_t rows = p.st->rows;
-    if (blockIdx.x == 0 && threadIdx.x == 0 && rows > 0) p.st->count_ns += globaltimer() - p.st->count_t0;
     const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
     for (int64_t g = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; g < rows; g += warps) expand_row(p, g, lane);
+    phase_end(&p.st->ph_e[kPhExpand]);
 }
 
 __global__ void __launch_bounds__(256) k_build_masks_g(const ResArgs* __restrict__ args) {
     const ResPtrs p = args->p;
+    phase_begin(&p.st->ph_s[kPhMasks]);
     build_masks(p);
+    phase_end(&p.st->ph_e[kPhMasks]);
 }
 
-__global__ void __launch_bounds__(256) k_index_mfis_g(const ResArgs* __restrict__ args) { index_mfis(args->p); }
-__global__ void __launch_bounds__(256) k_prune_stack_g(const ResArgs* __restrict__ args) { prune_stack(args->p); }
+__global__ void __launch_bounds__(256) k_index_mfis_g(const ResArgs* __restrict__ args) {
+    phase_begin(&args->p.st->ph_s[kPhMasks]);
+    index_mfis(args->p);
+    phase_end(&args->p.st->ph_e[kPhMasks]);
+}
+__global__ void __launch_bounds__(256) k_prune_stack_g(const ResArgs* __restrict__ args) {
+    phase_begin(&args->p.st->ph_s[kPhMasks]);
+    prune_stack(args->p);
+    phase_end(&args->p.st->ph_e[kPhMasks]);
+}
 
 __global__ void k_res_control(const ResArgs* __restrict__ args, cudaGraphConditionalHandle h) {
     if (threadIdx.x != 0) return;
@@ -1346,7 +1424,7 @@ int build_wave_graph(WaveGraph& G, const ResArgs* d_args, ResStatus* d_status, b
         if ((rc = launch_count_b1_persistent(&d_args->a1, &d_status->tiles_b1, &d_status->next1, sm * std::max(1, occ1), s)))
             break;
         if (with_proj &&
-            (rc = launch_count_proj_persistent(&d_args->a3, &d_status->n_proj, sm * std::max(1, occp), red_off, red_items, s)))
+            (rc = launch_count_proj_persistent(&d_args->ap, &d_status->n_proj, sm * std::max(1, occp), red_off, red_items, s)))
             break;
         k_res_expand_g<<<sm * std::max(1, occe), 256, 0, s>>>(d_args);
         k_build_masks_g<<<sm * 8, 256, 0, s>>>(d_args);
@@ -1399,6 +1477,7 @@ void free_resident(ResidentState* r, cudaStream_t s) {
 }
 
 int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
+    const auto t_entry = std::chrono::steady_clock::now();
     cudaStream_t s = c->stream;
     const int32_t d = c->n_counted;
     const int32_t minc = c->info.min_count;
@@ -1494,6 +1573,7 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
     top.sup = 0; top.next_row = n0; top.rows_done = 0; top.state = 0; top.top = 1;
     ResStatus hs;
     memset(&hs, 0, sizeof hs);
+    for (int k = 0; k < kPhases; k++) hs.ph_s[k] = ~0ull;
     hs.fam_n = 1;
     hs.item_n = n0;
     hs.jobs = 1;
@@ -1566,10 +1646,11 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
     // large families of the empty prefix: the tcgen05 kind::i8 counter, 128 x 128 tiles
     const bool top_i8 = top_b1 && o->counter != TFIM_COUNTER_TENSOR && n0 >= tn.i8_min_rows && n0 >= tn.i8_min_cols;
 
-    const double t_host0 = std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
     double sync_ms = 0, kernel_ms = 0;
     int64_t launches = 0, count_launches = 0, bytes_alg = 0, waves = 0;
+    int64_t path_launches[6] = {0, 0, 0, 0, 0, 0};
     const int64_t row_bytes = (c->n_bits + 7) / 8;
+    ResStatus* d_st = (ResStatus*)R.status.p;
 
     ResPtrs P;
     auto refresh_ptrs = [&]() {
@@ -1729,6 +1810,7 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
         CountArgs a;
         a.bitmap = c->d_bitmap; a.W = W; a.masks = c->d_masks.as<uint32_t>(); a.jobs = P.jobs; a.rows = P.rows;
         a.cols = P.items; a.out = P.counts;
+        stt->setup_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_entry).count();
         TFIM_CUDA(cudaEventRecord(c->ev0, s));
         if (top_mode == 2) {
             TFIM_TRY(launch_pair_count(c->d_red_off, c->d_red_items, c->n_bits, (const int32_t*)R.top_pos.p, n0, P.counts, s));
@@ -1762,12 +1844,10 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
         launches++;
         launches++;
         waves++;
-        float ms = 0;
-        TFIM_CUDA(cudaEventSynchronize(c->ev1));
-        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
-        kernel_ms += ms;
-        stt->top_ms += ms;
     }
+    // the counting path of the empty-prefix family, its work and (read at the end) its time
+    const int top_path = top_mode == 2 ? TFIM_PATH_PAIRS : top_i8 ? TFIM_PATH_TC : top_b1 ? TFIM_PATH_B1 : TFIM_PATH_LOP3;
+    path_launches[top_path]++;
     // following waves
     const bool use_graph = o->use_graphs != 0;
     int64_t host_waves = 0;
@@ -1788,9 +1868,14 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
             a.bitmap = c->d_bitmap; a.W = W; a.masks = P.masks; a.jobs = P.jobs; a.rows = P.rows;
             a.cols = P.items; a.out = P.counts; a.n_tiles = 0; a.job_list = P.proj_list;
             a.tiles = P.tiles_l3;
+            a.ph_s = &d_st->ph_s[kPhLop3]; a.ph_e = &d_st->ph_e[kPhLop3];
             ha->a3 = a;
             a.tiles = P.tiles_b1;
+            a.ph_s = &d_st->ph_s[kPhB1]; a.ph_e = &d_st->ph_e[kPhB1];
             ha->a1 = a;
+            a.tiles = P.tiles_l3;
+            a.ph_s = &d_st->ph_s[kPhProj]; a.ph_e = &d_st->ph_e[kPhProj];
+            ha->ap = a;
             TFIM_CUDA(cudaMemcpyAsync(d_args, ha, sizeof(ResArgs), cudaMemcpyHostToDevice, s));
             TFIM_CUDA(cudaGraphLaunch(R.graph.exec, s));
             launches++;
@@ -1810,7 +1895,9 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
         // per wave: pack, zero, lop3, b1, [proj], expand, masks, index, prune, control
         launches += (int64_t)hst->waves * (9 + (with_proj ? 1 : 0));
         count_launches += (int64_t)hst->waves * (2 + (with_proj ? 1 : 0));
-        kernel_ms += (double)hst->count_ns * 1e-6;
+        path_launches[TFIM_PATH_LOP3] += hst->waves;
+        path_launches[TFIM_PATH_B1] += hst->waves;
+        if (with_proj) path_launches[TFIM_PATH_PROJ] += hst->waves;
     }
     while (!use_graph) {
         k_res_pack<<<1, kPackThreads, 0, s>>>(P);
@@ -1830,27 +1917,31 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
         CountArgs a;
         a.bitmap = c->d_bitmap; a.W = W; a.masks = c->d_masks.as<uint32_t>(); a.jobs = P.jobs; a.rows = P.rows;
         a.cols = P.items; a.out = P.counts; a.job_list = P.proj_list;
-        TFIM_CUDA(cudaEventRecord(c->ev0, s));
         if (hst->tiles_l3) {
             a.tiles = P.tiles_l3;
             a.n_tiles = hst->tiles_l3;
+            a.ph_s = &d_st->ph_s[kPhLop3]; a.ph_e = &d_st->ph_e[kPhLop3];
             TFIM_TRY(launch_count_lop3(a, s));
             launches++;
             count_launches++;
+            path_launches[TFIM_PATH_LOP3]++;
         }
         if (hst->tiles_b1) {
             a.tiles = P.tiles_b1;
             a.n_tiles = hst->tiles_b1;
+            a.ph_s = &d_st->ph_s[kPhB1]; a.ph_e = &d_st->ph_e[kPhB1];
             TFIM_TRY(launch_count_b1(a, s));
             launches++;
             count_launches++;
+            path_launches[TFIM_PATH_B1]++;
         }
         if (hst->n_proj) {
+            a.ph_s = &d_st->ph_s[kPhProj]; a.ph_e = &d_st->ph_e[kPhProj];
             TFIM_TRY(launch_count_proj(a, P.proj_list, hst->n_proj, c->d_red_off, c->d_red_items, s));
             launches++;
             count_launches++;
+            path_launches[TFIM_PATH_PROJ]++;
         }
-        TFIM_CUDA(cudaEventRecord(c->ev1, s));
         const int64_t threads = (int64_t)hst->rows * 32;
         k_res_expand<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(P);
         TFIM_CUDA(cudaGetLastError());
@@ -1865,13 +1956,10 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
         launches++;
         launches++;
         host_waves++;
-        float ms = 0;
-        TFIM_CUDA(cudaEventSynchronize(c->ev1));
-        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
-        kernel_ms += ms;
     }
     waves += use_graph ? (int64_t)hst->waves : host_waves;
     // results
+    const auto t_read0 = std::chrono::steady_clock::now();
     const ResStatus fin = *hst;
     // the MFI pool through one pinned staging buffer: offsets, lengths, supports, items
     const size_t nm = (size_t)fin.mfi_n, ni = (size_t)fin.mfi_item_n;
@@ -1919,14 +2007,47 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
     stt->lookaheads_skipped += (int64_t)fin.skipped;
     stt->pruned_pep += (int64_t)fin.pep;
     stt->pruned_superset += (int64_t)fin.sup_pruned;
+    // device times: the empty-prefix family's counting (events) and every later wave's phases
+    // (stamps folded by the pack)
+    {
+        float top_ms = 0;
+        cudaEventElapsedTime(&top_ms, c->ev0, c->ev1);
+        stt->top_ms += top_ms;
+        kernel_ms += top_ms;
+        stt->path_ms[top_path] += top_ms;
+        stt->path_bytes[top_path] += bytes_alg;
+        stt->path_bitops[top_path] += top_mode == 2 ? 0 : (int64_t)n0 * (n0 + 1) / 2 * c->n_bits;
+        stt->path_supports[top_path] += top_out;
+        const double ns = 1e-6;
+        const int ph_of_path[5] = {kPhLop3, kPhB1, kPhTc, -1, kPhProj};
+        const int cls_of_path[5] = {kClsLop3, kClsB1, kClsTc, -1, kClsProj};
+        for (int q = 0; q < 5; q++) {
+            if (ph_of_path[q] >= 0) {
+                const double ms = (double)fin.ph_ns[ph_of_path[q]] * ns;
+                stt->path_ms[q] += ms;
+                kernel_ms += ms;
+            }
+            if (cls_of_path[q] >= 0) {
+                stt->path_bytes[q] += (int64_t)fin.cls_bytes[cls_of_path[q]];
+                stt->path_bitops[q] += (int64_t)fin.cls_bitops[cls_of_path[q]];
+                stt->path_supports[q] += (int64_t)fin.cls_sup[cls_of_path[q]];
+                bytes_alg += (int64_t)fin.cls_bytes[cls_of_path[q]];
+            }
+            stt->path_launches[q] += path_launches[q];
+        }
+        stt->pack_ms += (double)fin.ph_ns[kPhPack] * ns;
+        stt->zero_ms += (double)fin.ph_ns[kPhZero] * ns;
+        stt->expand_ms += (double)fin.ph_ns[kPhExpand] * ns;
+        stt->mask_ms += (double)fin.ph_ns[kPhMasks] * ns;
+    }
     stt->waves += waves;
     stt->launches += launches;
     stt->count_launches += count_launches;
     stt->kernel_ms += kernel_ms;
     stt->sync_ms += sync_ms;
-    stt->bytes_alg += bytes_alg + (int64_t)fin.bytes_alg;
+    stt->bytes_alg += bytes_alg;
     stt->bit_ops = stt->supports * c->n_bits;
-    (void)t_host0;
+    stt->readback_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_read0).count();
     return TFIM_OK;
 }
 

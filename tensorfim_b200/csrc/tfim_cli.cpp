@@ -226,7 +226,14 @@ int main(int argc, char** argv) {
            (long long)st.waves, (long long)st.nodes,
            (long long)st.supports, (long long)st.launches, (long long)st.lookaheads, (long long)st.lookahead_hits,
            (long long)st.pruned_pep);
-    printf("BMMA phase ms: mask=0 bmma=%g memcpy=0 scatter=0\n", st.kernel_ms);
+    // the reference's phase line (kernel_bmma.cu:985), measured: mask = prefix-mask building,
+    // bmma = counting kernels, memcpy = result read-back and ordering, scatter = the per-row
+    // expansion of counted rows into children and MFIs
+    printf("BMMA phase ms: mask=%g bmma=%g memcpy=%g scatter=%g\n", st.mask_ms, st.kernel_ms, st.readback_ms,
+           st.expand_ms);
+    printf("count path ms: lop3=%g b1=%g tc=%g pairs=%g proj=%g  pack=%g setup=%g\n", st.path_ms[TFIM_PATH_LOP3],
+           st.path_ms[TFIM_PATH_B1], st.path_ms[TFIM_PATH_TC], st.path_ms[TFIM_PATH_PAIRS], st.path_ms[TFIM_PATH_PROJ],
+           st.pack_ms, st.setup_ms);
     printf("======================================================================\n");
     tfim_close(ctx);
     if (proposal) tfim_mlp_free(proposal);

@@ -137,7 +137,26 @@ struct CountArgs {
     int32_t n_tiles;
     int32_t* out;
     const int32_t* job_list;   // projected counter: the jobs it counts
+    // phase stamps of the launch (or nullptr): the earliest block start and the latest block
+    // end, in %globaltimer nanoseconds (phase_begin / phase_end)
+    unsigned long long* ph_s = nullptr;
+    unsigned long long* ph_e = nullptr;
 };
+
+__device__ __forceinline__ unsigned long long dev_globaltimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Device time of a launch without any barrier: thread 0 of every block folds its start time
+// into *s (minimum) and its finish time into *e (maximum), so the phase runs from the first
+// block's start to the last block's end.  One atomic per block; a null pointer records nothing.
+__device__ __forceinline__ void phase_begin(unsigned long long* s) {
+    if (s && threadIdx.x == 0) atomicMin(s, dev_globaltimer());
+}
+__device__ __forceinline__ void phase_end(unsigned long long* e) {
+    if (e && threadIdx.x == 0) atomicMax(e, dev_globaltimer());
+}
 
 int launch_count_lop3(const CountArgs& a, cudaStream_t s);
 int launch_count_b1(const CountArgs& a, cudaStream_t s);

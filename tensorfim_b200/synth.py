@@ -16,7 +16,8 @@ from __future__ import annotations
 import dataclasses
 import numpy as np
 
-__all__ = ["Database", "CONFIGS", "generate", "write_fimi", "categorical", "replicate"]
+__all__ = ["Database", "CONFIGS", "CFG3_DEVIATION_MINSUP", "generate", "write_fimi", "write_fimi_replicated",
+           "categorical", "replicate", "cfg3_base"]
 
 
 @dataclasses.dataclass
@@ -109,6 +110,13 @@ def _cfg3_base(rng) -> tuple[list[np.ndarray], int]:
         w /= w.sum()
         probs.append(w[rng.permutation(int(k))])
     return probs, 49_000
+
+
+# The replicated 12.54M configuration at its specified 85% has no frequent item (its largest
+# item support is 0.711), so the dense benchmark runs the same generator with the minimum
+# support lowered to 6%: 271 frequent items, 40,760 nodes of the reference's search and
+# 31,589 MFIs.  This threshold is a labelled deviation from the specified 85%.
+CFG3_DEVIATION_MINSUP = 0.06
 
 
 def _cfg3(scale: float = 1.0, replicas: int = 256) -> Database:
@@ -208,6 +216,26 @@ CONFIGS = {1: _cfg1, 2: _cfg2, 3: _cfg3, 4: _cfg4, 5: _cfg5}
 
 def generate(cfg: int, **kw) -> Database:
     return CONFIGS[cfg](**kw)
+
+
+def cfg3_base() -> Database:
+    """The replicated configuration's 49,000 base rows (one replica)."""
+    return _cfg3(replicas=1)
+
+
+def write_fimi_replicated(path: str, base: Database, factor: int) -> None:
+    """The text of `factor` exact replicas of `base`, written as the base's text repeated
+    (the reference's replica construction, data/make_replica.py:22-31, concatenates copies
+    of the file in the same way)."""
+    import os
+    tmp = path + ".base"
+    write_fimi(tmp, base)
+    with open(tmp, "rb") as f:
+        blob = f.read()
+    os.unlink(tmp)
+    with open(path, "wb") as f:
+        for _ in range(factor):
+            f.write(blob)
 
 
 def write_fimi(path: str, db: Database, chunk_rows: int = 1 << 20) -> None:

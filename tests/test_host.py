@@ -160,3 +160,37 @@ def test_levelwise_generator_plants_patterns():
         s = support(rows, p)
         assert s == int(np.logical_and.reduce(bits[p], axis=0).sum())
         assert s >= int(0.001 * n)   # every pattern fires on at least 0.2% of rows in expectation
+
+
+def test_bench_reference_support_counts_match_the_oracle_search(oracle_mod):
+    """bench.py's reference-equivalent support counts are the reference search's node count x
+    survivors; the oracle runs that search (the replicated workload at its base size, where
+    the search is the same and only supports scale)."""
+    import bench
+    for name, db in (("cfg1", synth.generate(1)), ("cfg3dev", synth.cfg3_base())):
+        w = bench.WORKLOADS[name]
+        o = oracle_mod.OracleDB(None, w["minsup"], csr=(db.offsets, db.items))
+        o.mine(0)
+        assert o.nodes * o.info()["n_survivors"] == w["ref_supports"], name
+        o.close()
+
+
+def test_replicated_text_is_the_base_text_repeated(tmp_path):
+    base = synth.generate(3, replicas=1, scale=0.01)
+    p1, p2 = str(tmp_path / "a.txt"), str(tmp_path / "b.txt")
+    synth.write_fimi_replicated(p1, base, 3)
+    synth.write_fimi(p2, synth.replicate(base, 3))
+    assert open(p1, "rb").read() == open(p2, "rb").read()
+
+
+def test_path_rooflines_arithmetic():
+    from tensorfim_b200 import measure
+    st = {"path_ms": [2.0, 0, 1.0, 0, 0, 0], "path_launches": [2, 0, 1, 0, 0, 0],
+          "path_bytes": [4e9, 0, 1e9, 0, 0, 0], "path_bitops": [8e12, 0, 5e10, 0, 0, 0]}
+    p = measure.path_rooflines([st, st], hbm_gbs=6000.0, i8_macs=1e15)
+    assert set(p) == {"lop3", "tc"}
+    assert p["lop3"]["achieved_gbs"] == 2000.0 and p["lop3"]["launches"] == 4
+    assert abs(p["tc"]["tensor_frac"] - 0.05) < 1e-12
+    assert abs(p["lop3"]["share_of_counting"] - 2 / 3) < 1e-12
+    r = measure.headline_roofline(p, 6000.0, 1e15, "measured", "measured")
+    assert r["kernel"] == "k_count_lop3" and r["bound"] == "hbm" and abs(r["frac"] - 1 / 3) < 1e-12
