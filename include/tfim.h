@@ -363,7 +363,21 @@ TFIM_API int tfim_get_all(const tfim_ctx* ctx, int32_t* items, int64_t* offsets,
 TFIM_API int tfim_write_results(const tfim_ctx* ctx, const char* trans_set_file, const char* result_path,
                        double preprocessing_s, double computation_s);
 
+/*
+ * Free a database (the reference frees nothing: its device bitmap is a module global,
+ * code/engine/src/kernel_bitmap.cu:447-449).  The search's grown device pools (the resident
+ * engine's records and the prefix-mask pool) are kept for the next database opened on the
+ * same device, which adopts them instead of growing its own from their minimum; freed
+ * device blocks stay cached in the library's stream-ordered pool up to half the device's
+ * memory.
+ */
 TFIM_API void tfim_close(tfim_ctx* ctx);
+
+/*
+ * Free the device pools that closed databases left for reuse (see tfim_close), on
+ * `device`, or on every device when device < 0.  No counterpart in the reference.
+ */
+TFIM_API int tfim_release_cached(int32_t device);
 
 /* ------------------------------------------------------------------------------------
  * Learned lookahead proposal (no counterpart in the reference, which has no learned part).

@@ -46,7 +46,7 @@ EXPORTS = [
     "tfim_mlp_create", "tfim_mlp_num_params", "tfim_mlp_set_params", "tfim_mlp_get_params", "tfim_mlp_predict",
     "tfim_mlp_grad", "tfim_mlp_train", "tfim_mlp_free", "tfim_set_proposal", "tfim_lookahead_log",
     "tfim_tuning_get", "tfim_tuning_set", "tfim_tuning_load", "tfim_tuning_source",
-    "tfim_mine_all", "tfim_num_all", "tfim_all_item_total", "tfim_get_all",
+    "tfim_mine_all", "tfim_num_all", "tfim_all_item_total", "tfim_get_all", "tfim_release_cached",
 ]
 
 
@@ -149,6 +149,7 @@ def lib() -> C.CDLL:
     L.tfim_mine_opts_default.argtypes = [P(MineOpts)]
     L.tfim_mine_opts_default.restype = None
     L.tfim_mine.argtypes = [p, P(MineOpts), P(MineStats)]
+    L.tfim_release_cached.argtypes = [i32]
     L.tfim_num_mfis.argtypes = [p]
     L.tfim_num_mfis.restype = i64
     L.tfim_mfi_item_total.argtypes = [p]

@@ -514,12 +514,15 @@ int tfim_write_results(const tfim_ctx* c, const char* trans_set_file, const char
     return TFIM_OK;
 }
 
+int tfim_release_cached(int32_t device) { return tfim::release_cached(device); }
+
 void tfim_close(tfim_ctx* c) {
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->engine) tfim::free_engine(c->engine);
     c->engine = nullptr;
+    tfim::stash_resident(c);   // pools for the next database opened on this device
     if (c->resident) tfim::free_resident(c->resident, c->stream);
     c->resident = nullptr;
     tfim::dev_free(c->d_bitmap, c->stream);

@@ -38,7 +38,14 @@ cudaMemPool_t device_pool(int dev) {
             g_pools[dev] = nullptr;
             return nullptr;
         }
-        uint64_t keep = 16ull << 30;   // cached bytes kept across frees
+        // freed blocks stay cached in the pool up to half the device's memory, so that closing
+        // a database and opening the next one does not unmap and remap its buffers
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+            cudaGetLastError();
+            total_b = 32ull << 30;
+        }
+        uint64_t keep = (uint64_t)total_b / 2;
         cudaMemPoolSetAttribute(g_pools[dev], cudaMemPoolAttrReleaseThreshold, &keep);
     }
     return g_pools[dev];

@@ -1476,6 +1476,67 @@ void free_resident(ResidentState* r, cudaStream_t s) {
     delete r;
 }
 
+// Resident-engine pools and mask pools of closed contexts, one of each per device.  A
+// context that closes after its work has finished hands them over (its stream is idle); the
+// next context's first resident mine on that device adopts them, so a database opened again
+// starts from pools already grown to the last search's size instead of growing (and copying)
+// them from their minimum.  tfim_release_cached frees them.
+namespace {
+std::mutex g_cache_mu;
+ResidentState* g_cached_res[64] = {};
+DevBuf g_cached_masks[64];
+}  // namespace
+
+void stash_resident(tfim_ctx* c) {
+    const int dev = c->device;
+    if (dev < 0 || dev >= 64) return;
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    if (c->resident) {
+        c->resident->graph.release();   // its launches hold this context's transaction list
+        if (g_cached_res[dev]) free_resident(g_cached_res[dev], c->stream);
+        g_cached_res[dev] = c->resident;
+        c->resident = nullptr;
+    }
+    if (c->d_masks.p && c->d_masks.bytes > g_cached_masks[dev].bytes) {
+        g_cached_masks[dev].release();
+        g_cached_masks[dev] = c->d_masks;
+        c->d_masks.p = nullptr;
+        c->d_masks.bytes = 0;
+    }
+}
+
+void adopt_resident(tfim_ctx* c) {
+    const int dev = c->device;
+    if (dev < 0 || dev >= 64) return;
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    if (!c->resident && g_cached_res[dev]) {
+        c->resident = g_cached_res[dev];
+        g_cached_res[dev] = nullptr;
+    }
+    if (g_cached_masks[dev].p && g_cached_masks[dev].bytes > c->d_masks.bytes) {
+        c->d_masks.release();
+        c->d_masks = g_cached_masks[dev];
+        c->d_masks.stream = c->stream;
+        g_cached_masks[dev].p = nullptr;
+        g_cached_masks[dev].bytes = 0;
+    }
+}
+
+int release_cached(int dev) {
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    for (int d = 0; d < 64; d++) {
+        if (dev >= 0 && d != dev) continue;
+        if (!g_cached_res[d] && !g_cached_masks[d].p) continue;
+        TFIM_CUDA(cudaSetDevice(d));
+        if (g_cached_res[d]) free_resident(g_cached_res[d], nullptr);
+        g_cached_res[d] = nullptr;
+        g_cached_masks[d].stream = nullptr;
+        g_cached_masks[d].release();
+        TFIM_CUDA(cudaDeviceSynchronize());
+    }
+    return TFIM_OK;
+}
+
 int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
     const auto t_entry = std::chrono::steady_clock::now();
     cudaStream_t s = c->stream;
@@ -1484,6 +1545,7 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
     const int64_t W = c->W;
     const int32_t la_mode = o->lookahead;
     TFIM_CHECK(la_mode != 2 || c->proposal, TFIM_E_STATE, "lookahead mode 2 needs a proposal network (tfim_set_proposal)");
+    if (!c->resident) adopt_resident(c);
     if (!c->resident) c->resident = new ResidentState();
     ResidentState& R = *c->resident;
     c->la_feats.clear();

@@ -289,6 +289,10 @@ int mine_batched(tfim_ctx* ctx, const tfim_mine_opts* o, tfim_mine_stats* st);
 int mine_resident(tfim_ctx* ctx, const tfim_mine_opts* o, tfim_mine_stats* st);
 int mine_plain_roots(tfim_ctx* ctx, const std::vector<int32_t>& roots, tfim_mine_stats* st);
 void free_resident(ResidentState* r, cudaStream_t s);
+// Per-device cache of the resident pools and mask pool of closed contexts (resident.cu).
+void stash_resident(tfim_ctx* c);
+void adopt_resident(tfim_ctx* c);
+int release_cached(int device);
 int mlp_device_params(tfim_mlp* h, const void** wbf, const float** params);
 int compute_bit_supports(tfim_ctx* ctx);
 // Per-node prefix masks from item lists and one count job over every counted row (abi.cu):

@@ -313,6 +313,12 @@ class Database:
             pass
 
 
+def release_cached(device: int = -1) -> None:
+    """Free the device pools closed databases left for the next one (tfim_release_cached),
+    on `device` or on every device."""
+    check(lib().tfim_release_cached(int(device)))
+
+
 def result_path(path: str, minsup: float) -> str:
     """The reference's result-file name: sprintf("%s-%f=Results.txt") (kernel_bitmap.cu:906-907)."""
     return "%s-%f=Results.txt" % (path, minsup)

@@ -190,3 +190,19 @@ def test_large_top_family_on_every_tensor_path(oracle_mod, tmp_path):
         for counter in ("auto", "tensor", "lop3"):
             res = db.mine(engine="resident", counter=counter, top="bitmap", lookahead=False)
             assert res.as_dict() == exp, counter
+
+
+def test_pools_handed_to_the_next_database(tmp_path):
+    """A closed database leaves its grown pools for the next one opened on the device; the
+    next database (another word count per row, another search) adopts them and mines the
+    reference's MFIs, and so does one opened after the cache is released."""
+    names = ["cfg1_t03", "cfg4_s001", "cfg1_t03", "edge_ties"]
+    for k, name in enumerate(names):
+        fx = load_golden(name)
+        path = golden_input(fx, tmp_path)
+        with tf.Database.from_file(path, fx["spec"]["minsup"]) as db:
+            for graphs in (False, True):
+                assert db.mine(engine="resident", graphs=graphs).as_dict() == fx["expected"], (name, graphs)
+        if k == 2:
+            tf.release_cached()
+    tf.release_cached(0)
