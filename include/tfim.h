@@ -311,7 +311,11 @@ typedef struct {
     int32_t i8_min_cols;        /*   of at least i8_min_rows x i8_min_cols (tfim_count_wave and
                                      the empty-prefix family's bitmap Gram) */
     double  rate_i8_bitops;     /* cost model: tcgen05 kind::i8 bit-ops/s */
-    int32_t reserved[4];
+    int32_t tc_min_work;        /* automatic choice: the tcgen05 family counter for family jobs of
+                                   at most 128 columns with rows x columns >= tc_min_work and a */
+    float   tc_min_density;     /*   prefix holding at least this fraction of 128-bit positions */
+    float   tc_tiles_per_sm;    /* tcgen05 family counter: word-slice tiles per SM and wave */
+    int32_t reserved[1];
 } tfim_tuning;
 
 /* The table in force (built-in values, or the loaded / set table). */

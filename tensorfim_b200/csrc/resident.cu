@@ -53,9 +53,10 @@ enum { kJobFam = 0, kJobLook = 1 };
 struct DJob {
     int32_t fam, kind, r0, nr, slot, log;
     int32_t b3, b1;            // exclusive prefix of CUDA-core / tensor-core tiles over the wave's jobs
-    int32_t cls, sl3;          // counter (0 CUDA-core, 1 tensor-core, 2 projected); word slices of its CUDA-core tiles
+    int32_t cls, sl3;          // counter class (kCls*); word slices of its CUDA-core tiles
     int32_t b3l, heavy;        // CUDA-core tiles: heavy jobs' tiles come first (prefix b3), then the light
                                // jobs' (prefix b3l after all heavy tiles)
+    int32_t btc;               // exclusive prefix of the tcgen05 family counter's jobs
 };
 
 // Phases of a wave (device-time stamps) and counter classes of a count job.
@@ -72,6 +73,7 @@ struct ResStatus {
     int32_t grow, g_rows, g_jobs, g_max_head, g_max_cols, waves;
     int64_t g_out, g_tiles;
     int32_t launch_id, next3, next1, pad1;   // next3 / next1: tile counters of the persistent counters
+    int32_t tiles_tc, next_tc;               // tcgen05 family counter: tiles, tile counter
     unsigned long long launch_t0;
     unsigned long long supports, nodes, lookaheads, hits, skipped, pep;
     // superset check: MFIs [0, sup_done) are in the item -> MFI index the expand reads
@@ -122,6 +124,7 @@ struct ResPtrs {
     int32_t* row_local;
     TileDesc* tiles_l3;
     TileDesc* tiles_b1;
+    TileDesc* tiles_tc;
     int32_t* counts;
     // constants
     const uint32_t* bitmap;
@@ -147,6 +150,8 @@ struct ResPtrs {
     int32_t proj_auto;            // let the automatic counter choice pick the projected counter
     int32_t b1_min_rows, b1_min_cols;   // automatic choice: tensor path from this job shape
     float l3_slices_per_sm, b1_tiles_per_sm;   // work split targets per wave
+    int32_t tc_min_work;                       // automatic choice of the tcgen05 family counter
+    float tc_min_density, tc_tiles_per_sm;
     Caps caps;
     int64_t row_bytes;            // bytes of one bitmap row (algorithmic traffic accounting)
     const struct RowSum* row_sum; // first pass of the expand precomputed per wave row (or nullptr)
@@ -174,7 +179,7 @@ __host__ __device__ __forceinline__ int column_block(int nF) { return max(128, (
 // only rewrites this record (the captured launches stay valid).
 struct ResArgs {
     ResPtrs p;
-    CountArgs a3, a1, ap;   // CUDA-core, b1 and projected counters
+    CountArgs a3, a1, ap, atc;   // CUDA-core, b1, projected and tcgen05 family counters
 };
 
 __device__ __forceinline__ unsigned long long globaltimer() { return dev_globaltimer(); }
@@ -198,6 +203,19 @@ __host__ __device__ __forceinline__ int64_t lmax(int64_t a, int64_t b) { return 
 constexpr int kPackThreads = 1024;
 constexpr int kPackItems = 4;
 constexpr int kPackCand = kPackThreads * kPackItems;
+
+// The tcgen05 family counter takes a family job (its rows are a run of its columns) of at
+// most kFamMaxCols columns: always when that counter is asked for, and in the automatic choice
+// when the job is large enough and its prefix dense enough that skipping zero words (which
+// the CUDA-core tiles do and the tensor tiles do not) saves little.
+__device__ __forceinline__ bool use_tc(const ResPtrs& p, const JobDesc& jd, int32_t sup) {
+    if (jd.n_cols < 1 || jd.n_cols > kFamMaxCols || jd.n_rows < 1) return false;
+    if (p.counter == TFIM_COUNTER_I8) return true;
+    if (p.counter != TFIM_COUNTER_AUTO) return false;
+    if ((int64_t)jd.n_rows * jd.n_cols < p.tc_min_work) return false;
+    const float d = p.n_bits > 0 ? fminf(1.f, 128.f * (float)sup / (float)p.n_bits) : 1.f;
+    return d >= p.tc_min_density;
+}
 
 __device__ __forceinline__ bool use_b1_shape(const ResPtrs& p, int nr, int nc) {
     if (p.counter == TFIM_COUNTER_LOP3) return false;
@@ -229,7 +247,7 @@ __device__ __forceinline__ int find_job_by_tile(const DJob* dj, int nj, int64_t 
     int lo = 0, hi = nj - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
-        const int32_t v = K == 0 ? dj[mid].b3 : K == 1 ? dj[mid].b1 : dj[mid].b3l;
+        const int32_t v = K == 0 ? dj[mid].b3 : K == 1 ? dj[mid].b1 : K == 2 ? dj[mid].b3l : dj[mid].btc;
         if (v <= t) lo = mid; else hi = mid - 1;
     }
     return lo;
@@ -304,7 +322,7 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
             const DFam f = p.fams[L.fam];
             DJob dj;
             dj.fam = L.fam; dj.kind = kJobLook; dj.r0 = 0; dj.nr = 1; dj.slot = L.slot; dj.log = L.log; dj.b3 = 0; dj.b1 = 0;
-            dj.cls = 0; dj.sl3 = 1; dj.b3l = 0; dj.heavy = 0;
+            dj.cls = 0; dj.sl3 = 1; dj.b3l = 0; dj.heavy = 0; dj.btc = 0;
             p.djobs[k] = dj;
             JobDesc jd;
             jd.base_slot = -1; jd.base_item = -1; jd.n_rows = 1; jd.n_cols = f.nF - f.nT + 1;
@@ -408,7 +426,7 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
             const int32_t jid = s_n_jobs + (int32_t)hx[q];
             DJob dj;
             dj.fam = fid; dj.kind = kJobFam; dj.r0 = f.next_row; dj.nr = take[q]; dj.slot = -1; dj.log = -1; dj.b3 = 0; dj.b1 = 0;
-            dj.cls = 0; dj.sl3 = 1; dj.b3l = 0; dj.heavy = 0;
+            dj.cls = 0; dj.sl3 = 1; dj.b3l = 0; dj.heavy = 0; dj.btc = 0;
             p.djobs[jid] = dj;
             JobDesc jd;
             jd.base_slot = f.slot; jd.base_item = f.item; jd.n_rows = take[q]; jd.n_cols = f.nF;
@@ -464,23 +482,28 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
         return P4 * (1.f + d * (2.f + nr + nr * nc / 32.f));
     };
     float cost_local = 0.f;
-    int64_t tot1 = 0;
+    int64_t tot1 = 0, tottc = 0;
     for (int base = 0; base < nj; base += kPackCand) {
-        int64_t a1[kPackItems], x1[kPackItems];
+        int64_t a1[kPackItems], x1[kPackItems], at[kPackItems], xt[kPackItems];
         for (int q = 0; q < kPackItems; q++) {
             const int j = base + tid * kPackItems + q;
             a1[q] = 0;
+            at[q] = 0;
             if (j < nj) {
                 const JobDesc jd = p.jobs[j];
                 DJob* djp = p.djobs + j;
                 const bool fam = djp->kind == kJobFam;
-                int cls = 0;
-                if (fam && use_proj(p, jd, p.fams[djp->fam].sup)) {
-                    cls = 2;
+                const int32_t fsup = p.fams[djp->fam].sup;
+                int cls = kClsLop3;
+                if (fam && use_proj(p, jd, fsup)) {
+                    cls = kClsProj;
                     const int32_t k = atomicAdd(&p.st->n_proj, 1);
                     p.proj_list[k] = j;
+                } else if (fam && use_tc(p, jd, fsup)) {
+                    cls = kClsTc;
+                    at[q] = 1;
                 } else if (use_b1_shape(p, jd.n_rows, jd.n_cols) && fam) {
-                    cls = 1;
+                    cls = kClsB1;
                     a1[q] = b1_tiles(jd.n_rows, jd.n_cols);
                 } else {
                     cost_local += (float)l3_tiles(jd.n_rows, jd.n_cols) * l3_cost(jd, *djp);
@@ -491,11 +514,18 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
         Scan(tmp.scan).ExclusiveSum(a1, x1, s_agg);
         __syncthreads();
         const int64_t g1 = s_agg;
+        Scan(tmp.scan).ExclusiveSum(at, xt, s_agg);
+        __syncthreads();
+        const int64_t gt = s_agg;
         for (int q = 0; q < kPackItems; q++) {
             const int j = base + tid * kPackItems + q;
-            if (j < nj) p.djobs[j].b1 = (int32_t)(tot1 + x1[q]);
+            if (j < nj) {
+                p.djobs[j].b1 = (int32_t)(tot1 + x1[q]);
+                p.djobs[j].btc = (int32_t)(tottc + xt[q]);
+            }
         }
         tot1 += g1;
+        tottc += gt;
         __syncthreads();
     }
     __shared__ float s_cost;
@@ -557,9 +587,17 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
     if (kslice <= 0) kslice = 64;
     const int64_t nk = W > 0 ? (W + kslice - 1) / kslice : 1;
     const int64_t T3 = tot3, T1 = tot1 * nk;
+    // tcgen05 family tiles: every job whole, over `sltc` word slices (multiples of 64 words)
+    const int64_t want_tc = lmax(1, (int64_t)(p.tc_tiles_per_sm * (float)p.sm_count));
+    int64_t sltc = tottc > 0 ? lmax(1, (want_tc + tottc - 1) / tottc) : 1;
+    sltc = lmin(sltc, lmax(1, W / 64));
+    int64_t wsltc = ((W / 64 + sltc - 1) / sltc) * 64;
+    if (wsltc <= 0) wsltc = 64;
+    const int64_t ntc = W > 0 ? (W + wsltc - 1) / wsltc : 1;
+    const int64_t TT = tottc * ntc;
     // the wave is committed only when the worst case of its expand fits the pools
     if (tid == 0) {
-        const bool fit = s_out_total <= p.cap_out && T1 <= p.cap_tiles && T3 <= p.cap_tiles &&
+        const bool fit = s_out_total <= p.cap_out && T1 <= p.cap_tiles && T3 <= p.cap_tiles && TT <= p.cap_tiles &&
                          wave_fits(p.caps, *st, rows_total, nj, s_out_total, s_max_head, s_max_cols, p.log_on != 0);
         s_fit = fit;
         if (!fit) {
@@ -569,13 +607,14 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
             st->g_out = s_out_total;
             st->g_max_head = s_max_head;
             st->g_max_cols = s_max_cols;
-            st->g_tiles = lmax(T1, T3);
+            st->g_tiles = lmax(lmax(T1, T3), TT);
         }
     }
     __syncthreads();
     if (!s_fit) {
         if (tid == 0) {
-            st->jobs = 0; st->rows = 0; st->tiles_l3 = 0; st->tiles_b1 = 0; st->n_proj = 0; st->out_total = 0;
+            st->jobs = 0; st->rows = 0; st->tiles_l3 = 0; st->tiles_b1 = 0; st->tiles_tc = 0; st->n_proj = 0;
+            st->out_total = 0;
             st->ph_e[kPhPack] = globaltimer();
         }
         return;
@@ -651,11 +690,22 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
             p.tiles_b1[t] = TileDesc{j, rg * kB1Rows, min(kB1Rows, jd.n_rows - rg * kB1Rows), cc * kB1Cols,
                                      min(jd.n_cols, cc * kB1Cols + kB1Cols), (int32_t)w0, (int32_t)lmin(W, w0 + kslice), 0};
         }
+    if (TT <= p.cap_tiles)
+        for (int64_t t = tid; t < TT; t += kPackThreads) {
+            const int64_t slice = t / tottc, local = t % tottc;
+            const int j = find_job_by_tile<3>(p.djobs, nj, local);
+            const JobDesc jd = p.jobs[j];
+            const int64_t w0 = slice * wsltc;
+            // rows 0 .. n_rows of the job are its columns dj.r0 .. dj.r0 + n_rows
+            p.tiles_tc[t] = TileDesc{j, 0, jd.n_rows, 0, jd.n_cols, (int32_t)w0, (int32_t)lmin(W, w0 + wsltc),
+                                     p.djobs[j].r0};
+        }
     if (tid == 0) {
         st->jobs = nj;
         st->rows = rows_total;
         st->tiles_l3 = (int32_t)T3;
         st->tiles_b1 = (int32_t)T1;
+        st->tiles_tc = (int32_t)TT;
         st->out_total = s_out_total;
         st->max_cols = s_max_cols;
         st->max_head = s_max_head;
@@ -1311,6 +1361,7 @@ __global__ void __launch_bounds__(256) k_res_zero(const ResArgs* __restrict__ ar
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         st->next3 = 0;
         st->next1 = 0;
+        st->next_tc = 0;
     }
     const int64_t n = st->out_total;
     const int64_t n4 = n >> 2;
@@ -1403,6 +1454,7 @@ int build_wave_graph(WaveGraph& G, const ResArgs* d_args, ResStatus* d_status, b
     TFIM_CUDA(cudaGetDevice(&dev));
     TFIM_CUDA(cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, dev));
     TFIM_TRY(persistent_occupancy(&occ3, &occ1, &occp));
+    TFIM_TRY(configure_fam_kernel());
     TFIM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occe, k_res_expand_g, 256, 0));
     TFIM_CUDA(cudaGraphCreate(&G.graph, 0));
     cudaGraphConditionalHandle h;
@@ -1426,6 +1478,7 @@ int build_wave_graph(WaveGraph& G, const ResArgs* d_args, ResStatus* d_status, b
         if (with_proj &&
             (rc = launch_count_proj_persistent(&d_args->ap, &d_status->n_proj, sm * std::max(1, occp), red_off, red_items, s)))
             break;
+        if ((rc = launch_count_fam_persistent(&d_args->atc, &d_status->tiles_tc, &d_status->next_tc, sm, s))) break;
         k_res_expand_g<<<sm * std::max(1, occe), 256, 0, s>>>(d_args);
         k_build_masks_g<<<sm * 8, 256, 0, s>>>(d_args);
         k_index_mfis_g<<<sm, 256, 0, s>>>(d_args);
@@ -1448,15 +1501,15 @@ int build_wave_graph(WaveGraph& G, const ResArgs* d_args, ResStatus* d_status, b
 
 struct ResidentState {
     Pool fams, items, heads, stack, looks, free_slots, defer, mfi_off, mfi_len, mfi_sup, mfi_items, log_feat, log_label;
-    Pool djobs, jobs, rows, row_job, row_local, tiles_l3, tiles_b1, counts, status, is_root, dense_freq, top_pos, top_diag,
-        proj_list, args, top_sum, mjobs, sup_index;
+    Pool djobs, jobs, rows, row_job, row_local, tiles_l3, tiles_b1, tiles_tc, counts, status, is_root, dense_freq, top_pos,
+        top_diag, proj_list, args, top_sum, mjobs, sup_index;
     HostBuf h_status, h_args, h_res, h_setup;
     WaveGraph graph;
     int32_t launch_id = 0;
     void release(cudaStream_t s) {
         graph.release();
         for (Pool* b : {&fams, &items, &heads, &stack, &looks, &free_slots, &defer, &mfi_off, &mfi_len, &mfi_sup, &mfi_items,
-                        &log_feat, &log_label, &djobs, &jobs, &rows, &row_job, &row_local, &tiles_l3, &tiles_b1, &counts,
+                        &log_feat, &log_label, &djobs, &jobs, &rows, &row_job, &row_local, &tiles_l3, &tiles_b1, &tiles_tc, &counts,
                         &status, &is_root, &dense_freq, &top_pos, &top_diag, &proj_list, &args, &top_sum, &mjobs,
                         &sup_index}) {
             dev_free(b->p, s);
@@ -1610,6 +1663,7 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
     TFIM_TRY(grow(R.mjobs, (2 * cap_rows + 2) * sizeof(MaskJob), s));   // at most two masks per expanded row
     TFIM_TRY(grow(R.tiles_l3, cap_tiles * sizeof(TileDesc), s));
     TFIM_TRY(grow(R.tiles_b1, cap_tiles * sizeof(TileDesc), s));
+    TFIM_TRY(grow(R.tiles_tc, cap_tiles * sizeof(TileDesc), s));
     TFIM_TRY(grow(R.counts, cap_out * 4, s));
     TFIM_TRY(grow(R.is_root, is_root.size(), s));
     TFIM_TRY(grow(R.dense_freq, (size_t)std::max<int32_t>(c->info.n_dense, 1) * 4, s));
@@ -1711,6 +1765,7 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
     double sync_ms = 0, kernel_ms = 0;
     int64_t launches = 0, count_launches = 0, bytes_alg = 0, waves = 0;
     int64_t path_launches[6] = {0, 0, 0, 0, 0, 0};
+    bool used_tc = false;   // the tcgen05 family counter ran (its error flag is read at the end)
     const int64_t row_bytes = (c->n_bits + 7) / 8;
     ResStatus* d_st = (ResStatus*)R.status.p;
 
@@ -1724,7 +1779,8 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
         P.djobs = (DJob*)R.djobs.p; P.jobs = (JobDesc*)R.jobs.p; P.rows = (RowDesc*)R.rows.p;
         P.mjobs = (MaskJob*)R.mjobs.p;
         P.row_job = (int32_t*)R.row_job.p; P.row_local = (int32_t*)R.row_local.p;
-        P.tiles_l3 = (TileDesc*)R.tiles_l3.p; P.tiles_b1 = (TileDesc*)R.tiles_b1.p; P.counts = (int32_t*)R.counts.p;
+        P.tiles_l3 = (TileDesc*)R.tiles_l3.p; P.tiles_b1 = (TileDesc*)R.tiles_b1.p; P.tiles_tc = (TileDesc*)R.tiles_tc.p;
+        P.counts = (int32_t*)R.counts.p;
         P.bitmap = c->d_bitmap; P.masks = c->d_masks.as<uint32_t>(); P.dense_freq = (const int32_t*)R.dense_freq.p;
         P.is_root = (const uint8_t*)R.is_root.p; P.st = (ResStatus*)R.status.p;
         P.W = W; P.n_bits = c->n_bits; P.min_count = minc; P.wave_rows = wave_rows;
@@ -1739,6 +1795,9 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
         P.b1_min_cols = tn.b1_min_cols;
         P.l3_slices_per_sm = tn.l3_slices_per_sm;
         P.b1_tiles_per_sm = tn.b1_tiles_per_sm;
+        P.tc_min_work = tn.tc_min_work;
+        P.tc_min_density = tn.tc_min_density;
+        P.tc_tiles_per_sm = tn.tc_tiles_per_sm;
         if (la_mode == 2 && c->proposal) {
             const void* wb = nullptr;
             const float* pp = nullptr;
@@ -1822,6 +1881,7 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
                 cap_tiles = std::max<int64_t>(2 * cap_tiles, h.g_tiles);
                 TFIM_TRY(grow(R.tiles_l3, cap_tiles * sizeof(TileDesc), s));
                 TFIM_TRY(grow(R.tiles_b1, cap_tiles * sizeof(TileDesc), s));
+                TFIM_TRY(grow(R.tiles_tc, cap_tiles * sizeof(TileDesc), s));
             }
             TFIM_TRY(ensure(h, h.g_rows, h.g_jobs, h.g_out, h.g_max_head, h.g_max_cols));
         }
@@ -1863,6 +1923,7 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
             cap_tiles = (int64_t)tl.size();
             TFIM_TRY(grow(R.tiles_l3, cap_tiles * sizeof(TileDesc), s));
             TFIM_TRY(grow(R.tiles_b1, cap_tiles * sizeof(TileDesc), s));
+            TFIM_TRY(grow(R.tiles_tc, cap_tiles * sizeof(TileDesc), s));
             refresh_ptrs();
         }
         if (!tl.empty())
@@ -1938,6 +1999,9 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
             a.tiles = P.tiles_l3;
             a.ph_s = &d_st->ph_s[kPhProj]; a.ph_e = &d_st->ph_e[kPhProj];
             ha->ap = a;
+            a.tiles = P.tiles_tc;
+            a.ph_s = &d_st->ph_s[kPhTc]; a.ph_e = &d_st->ph_e[kPhTc];
+            ha->atc = a;
             TFIM_CUDA(cudaMemcpyAsync(d_args, ha, sizeof(ResArgs), cudaMemcpyHostToDevice, s));
             TFIM_CUDA(cudaGraphLaunch(R.graph.exec, s));
             launches++;
@@ -1954,11 +2018,13 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
             if (hst->jobs == 0) break;   // the stack and the lookahead queue are empty
             TFIM_CHECK(slices < (1LL << 40), TFIM_E_STATE, "resident search did not finish");
         }
-        // per wave: pack, zero, lop3, b1, [proj], expand, masks, index, prune, control
-        launches += (int64_t)hst->waves * (9 + (with_proj ? 1 : 0));
-        count_launches += (int64_t)hst->waves * (2 + (with_proj ? 1 : 0));
+        // per wave: pack, zero, lop3, b1, [proj], tc, expand, masks, index, prune, control
+        launches += (int64_t)hst->waves * (10 + (with_proj ? 1 : 0));
+        count_launches += (int64_t)hst->waves * (3 + (with_proj ? 1 : 0));
         path_launches[TFIM_PATH_LOP3] += hst->waves;
         path_launches[TFIM_PATH_B1] += hst->waves;
+        path_launches[TFIM_PATH_TC] += hst->waves;
+        used_tc = true;
         if (with_proj) path_launches[TFIM_PATH_PROJ] += hst->waves;
     }
     while (!use_graph) {
@@ -1996,6 +2062,16 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
             launches++;
             count_launches++;
             path_launches[TFIM_PATH_B1]++;
+        }
+        if (hst->tiles_tc) {
+            a.tiles = P.tiles_tc;
+            a.n_tiles = hst->tiles_tc;
+            a.ph_s = &d_st->ph_s[kPhTc]; a.ph_e = &d_st->ph_e[kPhTc];
+            TFIM_TRY(launch_count_fam(a, s));
+            launches++;
+            count_launches++;
+            path_launches[TFIM_PATH_TC]++;
+            used_tc = true;
         }
         if (hst->n_proj) {
             a.ph_s = &d_st->ph_s[kPhProj]; a.ph_e = &d_st->ph_e[kPhProj];
@@ -2044,6 +2120,7 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
     }
     TFIM_CUDA(cudaStreamSynchronize(s));
     if (top_i8 && top_mode == 1) TFIM_TRY(count_i8_status(true));
+    if (used_tc) TFIM_TRY(count_fam_status(true));
     {
         MfiSet& M = c->mfis;
         const size_t base = M.items.size();

@@ -176,6 +176,16 @@ int configure_count_kernels();
 // `reset` clears) the device flag the kernel sets when an mbarrier wait expired.
 int launch_count_i8(const CountArgs& a, cudaStream_t s);
 int count_i8_status(bool reset);
+// tcgen05 kind::i8 family counter (count_fam.cu): a tile is one family job (rows a run of its
+// columns, at most kFamMaxCols columns) over a word slice, TileDesc.pad = the F position of
+// the tile's first row; one CTA per SM.  The persistent form reads its arguments and tile
+// count from device memory and takes tiles from `d_next` (zero at launch).
+constexpr int kFamMaxCols = 128;
+int launch_count_fam(const CountArgs& a, cudaStream_t s);
+int launch_count_fam_persistent(const CountArgs* d_args, const int32_t* d_n_tiles, int32_t* d_next, int32_t grid,
+                                cudaStream_t s);
+int count_fam_status(bool reset);
+int configure_fam_kernel();   // opt into its shared memory (once per device, before any capture)
 // The tuning table in force (common.cu): built-in values, or the table loaded / set.
 tfim_tuning tuning();
 int launch_pair_count(const int64_t* red_off, const int32_t* red_items, int64_t n_red, const int32_t* pos,

@@ -34,6 +34,9 @@ VARIANTS = [
     dict(engine="resident", counter="tensor", lookahead="all", wave_cap=37, graphs=True),
     dict(engine="resident", counter="lop3", lookahead="learned", top="bitmap", graphs=True),
     dict(engine="resident", counter="proj", lookahead="all", wave_cap=29, graphs=True),
+    dict(engine="resident", counter="i8", lookahead="learned"),
+    dict(engine="resident", counter="i8", lookahead="all", wave_cap=37, graphs=True),
+    dict(engine="resident", counter="i8", lookahead=False, top="bitmap", small_pools=True),
 ]
 PLAIN_OK = {"cfg1_full", "cfg2_full", "cfg3_base", "cfg3_base_t30", "cfg4_s001", "cfg5_s002", "edge_dups",
             "edge_format", "edge_identical", "edge_item0", "edge_none", "edge_single", "edge_ties"}
