@@ -1553,6 +1553,9 @@ void stash_resident(tfim_ctx* c) {
     if (c->d_masks.p && c->d_masks.bytes > g_cached_masks[dev].bytes) {
         g_cached_masks[dev].release();
         g_cached_masks[dev] = c->d_masks;
+        // the closing context's stream is idle and about to be destroyed: a cached buffer
+        // holds no stream (freed on the default stream, adopted onto the adopter's)
+        g_cached_masks[dev].stream = nullptr;
         c->d_masks.p = nullptr;
         c->d_masks.bytes = 0;
     }
