@@ -16,18 +16,24 @@
 // s0 & ~7 (8-row groups keep the 128-byte swizzle phase) and spans N = roundup16 of what
 // it must cover, at most 144 rows, so the expanded stage holds 144 rows.
 //
-// Warp roles (288 threads, one CTA per SM, persistent over a tile counter):
+// Warp roles (320 threads, one CTA per SM, persistent over a tile counter):
 //   warp 0     : one lane issues the stage's 8 MMAs (K = 32 bytes each, 2 K blocks of
 //                128 bits) once the stage is full, and commits them to the stage's `empty`
 //                barrier; after the tile's last stage it commits to `done`;
-//   warps 1..8 : X rows r = warp-1 (mod 8): raw bit words are prefetched with cp.async eight
-//                stages ahead into a warp-private ring (rows and the base's one or two
-//                sources), ANDed with the base, expanded (byte lane b of output word 8q+i is
-//                bit i+8b of input word q; any K order shared by both operands works) and
-//                stored in the K-major 128-byte-swizzle layout; each warp arrives on the
-//                stage's `full` barrier; warps 1..4 then read the accumulator (tcgen05.ld,
-//                32 lanes each) and add the counts to the job's output with int32 atomics
-//                (word slices of one job meet there).
+//   warp 9     : the loader: the raw bit words of a chunk of stages -- every X row's item
+//                row and the base's one or two sources, C stages of 256 bits each -- come
+//                into a three-slot ring with one bulk copy (cp.async.bulk, the TMA engine's
+//                untiled copy of this GPU's own memory) per row and chunk, completing on
+//                the slot's transaction-count barrier.  A chunk is about 24 KiB whatever
+//                the family's width (C = 5 stages at 130 rows, 42 at 18), so about 72 KiB
+//                are in flight per SM;
+//   warps 1..8 : X rows r = warp-1 (mod 8): the stage's raw words, ANDed with the base, are
+//                expanded (byte lane b of output word 8q+i is bit i+8b of input word q; any K
+//                order shared by both operands works) and stored in the K-major
+//                128-byte-swizzle layout; each warp arrives on the stage's `full` barrier and,
+//                after a chunk's last stage, on the slot's `rempty` barrier; warps 1..4 then
+//                read the accumulator (tcgen05.ld, 32 lanes each) and add the counts to the
+//                job's output with int32 atomics (word slices of one job meet there).
 // Every mbarrier wait is bounded; on expiry the kernel records an error, stops issuing,
 // drains what it issued and frees its tensor memory.
 #include <atomic>
@@ -45,15 +51,17 @@ constexpr int kFBlockBytes = kFXRows * kFKBytes;       // 18 KiB (a multiple of 
 constexpr int kFStageBytes = kFKBlocks * kFBlockBytes; // 36 KiB
 constexpr int kFStages = 4;
 constexpr int kFExpWarps = 8;
-constexpr int kFThreads = 32 * (1 + kFExpWarps);
-constexpr int kFRowsPerWarp = kFM / kFExpWarps;        // 16
-constexpr int kFRaw = 8;                               // raw prefetch depth, stages
-constexpr int kFRawEntries = kFRowsPerWarp + 2;        // rows + up to two base sources
+constexpr int kFLoadWarp = 1 + kFExpWarps;             // warp 9
+constexpr int kFThreads = 32 * (2 + kFExpWarps);       // 320
 constexpr int kFStageWords = kFKBlocks * kFKBytes / 32;   // 8 words of 32 bits per row per stage
-constexpr int kFRawWarpBytes = kFRaw * kFRawEntries * kFStageWords * 4;   // 4608
-constexpr int kFSmem = kFStages * kFStageBytes + kFExpWarps * kFRawWarpBytes + 1024;
+constexpr int kFStageRaw = kFStageWords * 4;           // 32 raw bytes per row per stage
+constexpr int kFRawSlots = 3;
+constexpr int kFRawSlotBytes = 24 * 1024;              // one chunk of raw rows
+constexpr int kFMaxEntries = kFM + 2;                  // rows + up to two base sources
+constexpr int kFSmem = kFStages * kFStageBytes + kFRawSlots * kFRawSlotBytes + 1024;
 constexpr uint32_t kFTmemCols = 256;
 constexpr uint32_t kFSpin = 1u << 22;
+static_assert(kFRawSlotBytes / (kFMaxEntries * kFStageRaw) >= 1, "a chunk holds at least one stage");
 
 __device__ int g_fam_status;   // 0 ok, 1 an mbarrier wait expired
 
@@ -63,12 +71,17 @@ __device__ __forceinline__ void st_shared_v4(uint32_t addr, uint32_t a, uint32_t
     asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(a), "r"(b), "r"(c), "r"(d) : "memory");
 }
 
-__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+// Bulk copy of `bytes` (a multiple of 16, both addresses 16-byte aligned) from this GPU's
+// global memory into shared memory, completing on the barrier's transaction count.
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(bar), "r"(bytes)
+                 : "memory");
+}
 
 // K-major, 128-byte swizzle shared-memory matrix descriptor: start address, leading byte
 // offset 16 (unused by swizzled K-major layouts), stride byte offset 1024 (8-row groups),
@@ -138,9 +151,10 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
 }
 
 struct FamShared {
-    uint64_t full[kFStages], empty[kFStages], done;
+    uint64_t full[kFStages], empty[kFStages], done, rfull[kFRawSlots], rempty[kFRawSlots];
     uint32_t tmem;
     int32_t tile, abort;
+    const uint32_t* src[kFMaxEntries];   // raw sources of the tile: X rows, then the base's
 };
 
 // a_dev (device copy of the arguments, read when non-null: a graph's launches outlive pool
@@ -163,6 +177,10 @@ __global__ void __launch_bounds__(kFThreads, 1) k_count_fam(CountArgs a_val, con
             mbar_init(smem_u32(&sh.full[s]), kFExpWarps);
             mbar_init(smem_u32(&sh.empty[s]), 1);
         }
+        for (int s = 0; s < kFRawSlots; s++) {
+            mbar_init(smem_u32(&sh.rfull[s]), 1);
+            mbar_init(smem_u32(&sh.rempty[s]), kFExpWarps);
+        }
         mbar_init(smem_u32(&sh.done), 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         sh.abort = 0;
@@ -177,7 +195,8 @@ __global__ void __launch_bounds__(kFThreads, 1) k_count_fam(CountArgs a_val, con
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = sh.tmem;
 
-    uint32_t g = 0;        // stages issued by this CTA before the current tile (barrier phases)
+    uint32_t g = 0;        // stages of the CTA before the current tile (phases of full / empty)
+    uint32_t gc = 0;       // raw chunks of the CTA before the current tile (phases of rfull / rempty)
     uint32_t n_done = 0;   // tiles finished (phase of `done`)
     bool first = true;
     while (true) {
@@ -199,6 +218,20 @@ __global__ void __launch_bounds__(kFThreads, 1) k_count_fam(CountArgs a_val, con
         const int ncov = s0 + t.nr - b8;
         const int N = (ncov + 15) & ~15;           // 16 .. 144
         const int n_st = (t.w1 - t.w0) / kFStageWords;
+        const int nbase = (j.base_slot >= 0 ? 1 : 0) + (j.base_item >= 0 ? 1 : 0);
+        const int n_ent = nF + nbase;
+        // stages per raw chunk: a chunk of every entry fits one ring slot
+        const int C = max(1, kFRawSlotBytes / (n_ent * kFStageRaw));
+        const int n_chunks = (n_st + C - 1) / C;
+        // the tile's raw sources
+        for (int q = tid; q < n_ent; q += kFThreads) {
+            const uint32_t* p;
+            if (q < nF) p = a.bitmap + (int64_t)a.cols[j.col_off + q] * W;
+            else if (q == nF && j.base_slot >= 0) p = a.masks + (int64_t)j.base_slot * W;
+            else p = a.bitmap + (int64_t)j.base_item * W;
+            sh.src[q] = p;
+        }
+        __syncthreads();
 
         if (warp == 0) {
             if (lane == 0) {
@@ -233,33 +266,33 @@ __global__ void __launch_bounds__(kFThreads, 1) k_count_fam(CountArgs a_val, con
                 tc_commit(smem_u32(&sh.done));
             }
             __syncwarp();
+        } else if (warp == kFLoadWarp) {
+            // ---- loader: chunk k of the tile into slot (gc + k) % kFRawSlots
+            bool ok = true;
+            for (int k = 0; k < n_chunks; k++) {
+                const uint32_t ck = gc + (uint32_t)k;
+                const int slot = (int)(ck % kFRawSlots);
+                if (ck >= (uint32_t)kFRawSlots) ok = mbar_wait(smem_u32(&sh.rempty[slot]), ((ck / kFRawSlots) - 1u) & 1u);
+                ok = __all_sync(0xffffffffu, ok);
+                if (!ok) break;
+                const int st0 = k * C, ns = min(C, n_st - st0);
+                const uint32_t bytes = (uint32_t)ns * kFStageRaw;   // per entry, a multiple of 32
+                const uint32_t bar = smem_u32(&sh.rfull[slot]);
+                if (lane == 0) mbar_expect_tx(bar, bytes * (uint32_t)n_ent);
+                __syncwarp();
+                const uint32_t dst0 = raw_base + (uint32_t)slot * kFRawSlotBytes;
+                const int64_t w = t.w0 + (int64_t)st0 * kFStageWords;
+                for (int q = lane; q < n_ent; q += 32)
+                    bulk_load(dst0 + (uint32_t)(q * C * kFStageRaw), sh.src[q] + w, bytes, bar);
+            }
+            if (!ok && lane == 0) {
+                atomicExch(&sh.abort, 1);
+                atomicExch(&g_fam_status, 1);
+            }
         } else {
-            // ---- loads and expansion: X rows r = e, e + 8, ... (< nF)
+            // ---- expansion: X rows r = e, e + 8, ... (< nF)
             const int e = warp - 1;
             const int nrw = nF > e ? (nF - e + kFExpWarps - 1) / kFExpWarps : 0;
-            const uint32_t* base_m = j.base_slot >= 0 ? a.masks + (int64_t)j.base_slot * W : nullptr;
-            const uint32_t* base_i = j.base_item >= 0 ? a.bitmap + (int64_t)j.base_item * W : nullptr;
-            const int nbase = (base_m ? 1 : 0) + (base_i ? 1 : 0);
-            const int n_ent = nrw + nbase;
-            const uint32_t wraw = raw_base + (uint32_t)e * kFRawWarpBytes;
-            // entry q: rows 0 .. nrw-1, then the base sources
-            auto src_of = [&](int q) -> const uint32_t* {
-                if (q < nrw) return a.bitmap + (int64_t)a.cols[j.col_off + e + q * kFExpWarps] * W;
-                const int b = q - nrw;
-                return (b == 0 && base_m) ? base_m : base_i;
-            };
-            auto issue = [&](int st) {
-                if (st < n_st) {
-                    const int64_t w = t.w0 + (int64_t)st * kFStageWords;
-                    const uint32_t dst0 = wraw + (uint32_t)((st % kFRaw) * kFRawEntries * kFStageWords * 4);
-                    for (int u = lane; u < 2 * n_ent; u += 32) {
-                        const int q = u >> 1, h = u & 1;
-                        cp_async16(dst0 + (uint32_t)(q * kFStageWords * 4 + h * 16), src_of(q) + w + h * 4);
-                    }
-                }
-                cp_async_commit();
-            };
-            for (int p = 0; p < kFRaw - 1; p++) issue(p);
             bool ok = true;
             // lane -> (row of the pass, 16-byte output chunk): 2 rows per pass, 16 chunks per row
             const int half = lane >> 4, chunk = lane & 15;
@@ -267,34 +300,33 @@ __global__ void __launch_bounds__(kFThreads, 1) k_count_fam(CountArgs a_val, con
             const int qw = kb * 4 + (c >> 1);   // input word of this chunk within the stage
             const int sh0 = 4 * (c & 1);
             for (int st = 0; st < n_st; st++) {
-                issue(st + kFRaw - 1);
-                cp_async_wait<kFRaw - 1>();
-                __syncwarp();
+                const int k = st / C, within = st - k * C;
+                const uint32_t ck = gc + (uint32_t)k;
+                const int slot = (int)(ck % kFRawSlots);
+                if (within == 0 && ok) ok = mbar_wait(smem_u32(&sh.rfull[slot]), (ck / kFRawSlots) & 1u);
                 const uint32_t it = g + (uint32_t)st;
                 const int s = (int)(it % kFStages);
                 if (ok && it >= (uint32_t)kFStages)
                     ok = mbar_wait(smem_u32(&sh.empty[s]), ((it / kFStages) - 1u) & 1u);
                 ok = __all_sync(0xffffffffu, ok);
                 if (!ok) break;
-                const uint32_t rs = wraw + (uint32_t)((st % kFRaw) * kFRawEntries * kFStageWords * 4);
+                // raw word qw of entry q at stage `within` of the slot
+                const uint32_t rs = raw_base + (uint32_t)slot * kFRawSlotBytes + (uint32_t)(within * kFStageRaw + qw * 4);
+                const uint32_t ent = (uint32_t)(C * kFStageRaw);
                 uint32_t bw = ~0u;
-                if (nbase > 0) {
+                for (int b = 0; b < nbase; b++) {
                     uint32_t x;
-                    asm volatile("ld.shared.b32 %0, [%1];" : "=r"(x) : "r"(rs + (uint32_t)((nrw * kFStageWords + qw) * 4)));
-                    bw = x;
-                    if (nbase > 1) {
-                        asm volatile("ld.shared.b32 %0, [%1];" : "=r"(x) : "r"(rs + (uint32_t)(((nrw + 1) * kFStageWords + qw) * 4)));
-                        bw &= x;
-                    }
+                    asm volatile("ld.shared.b32 %0, [%1];" : "=r"(x) : "r"(rs + (uint32_t)(nF + b) * ent));
+                    bw &= x;
                 }
                 const uint32_t stage = base + (uint32_t)s * kFStageBytes + (uint32_t)kb * kFBlockBytes;
                 for (int q0 = 0; q0 < nrw; q0 += 2) {
                     const int q = q0 + half;
                     if (q < nrw) {
-                        uint32_t x;
-                        asm volatile("ld.shared.b32 %0, [%1];" : "=r"(x) : "r"(rs + (uint32_t)((q * kFStageWords + qw) * 4)));
-                        x = (x & bw) >> sh0;
                         const int r = e + q * kFExpWarps;
+                        uint32_t x;
+                        asm volatile("ld.shared.b32 %0, [%1];" : "=r"(x) : "r"(rs + (uint32_t)r * ent));
+                        x = (x & bw) >> sh0;
                         st_shared_v4(stage + (uint32_t)r * kFKBytes + (uint32_t)((c ^ (r & 7)) << 4), x & 0x01010101u,
                                      (x >> 1) & 0x01010101u, (x >> 2) & 0x01010101u, (x >> 3) & 0x01010101u);
                     }
@@ -302,9 +334,11 @@ __global__ void __launch_bounds__(kFThreads, 1) k_count_fam(CountArgs a_val, con
                 // generic-proxy stores -> visible to the tensor cores' async proxy
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 __syncwarp();
-                if (lane == 0) mbar_arrive(smem_u32(&sh.full[s]));
+                if (lane == 0) {
+                    mbar_arrive(smem_u32(&sh.full[s]));
+                    if (within == C - 1 || st == n_st - 1) mbar_arrive(smem_u32(&sh.rempty[slot]));
+                }
             }
-            cp_async_wait<0>();
             if (!ok && lane == 0) {
                 atomicExch(&sh.abort, 1);
                 atomicExch(&g_fam_status, 1);
@@ -313,12 +347,12 @@ __global__ void __launch_bounds__(kFThreads, 1) k_count_fam(CountArgs a_val, con
             if (warp <= 4) {
                 const bool fin = mbar_wait(smem_u32(&sh.done), n_done & 1u);
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const bool good = __all_sync(0xffffffffu, fin) && !sh.abort && n_st > 0;
-                if (!__all_sync(0xffffffffu, fin) && lane == 0) {
+                const bool all_fin = __all_sync(0xffffffffu, fin);
+                if (!all_fin && lane == 0) {
                     atomicExch(&sh.abort, 1);
                     atomicExch(&g_fam_status, 1);
                 }
-                if (good) {
+                if (all_fin && !sh.abort && n_st > 0) {
                     const int lq = warp & 3;
                     const int col = 32 * lq + lane;
                     for (int n0 = 0; n0 < N; n0 += 16) {
@@ -339,9 +373,10 @@ __global__ void __launch_bounds__(kFThreads, 1) k_count_fam(CountArgs a_val, con
             }
         }
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        __syncthreads();   // accumulator read, stages and tables free for the next tile
+        __syncthreads();   // accumulator read, stages, ring and tables free for the next tile
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         g += (uint32_t)max(n_st, 0);
+        gc += (uint32_t)n_chunks;
         n_done++;
     }
     __syncthreads();

@@ -2,7 +2,7 @@
 
     python -m tensorfim_b200.profcase --cfg 4 --scale 0.25 --counter tensor [--engine batched|resident|plain]
                                       [--top auto|bitmap|pairs] [--lookahead off|filtered|learned|all]
-                                      [--graphs] [--repeat N]
+                                      [--graphs] [--repeat N] [--minsup F] [--replicas R]
 
 Generates the configuration's database (tensorfim_b200.synth) at the given row scale,
 builds it on cuda:0 and mines it once; prints the MFI count and the engine statistics.
@@ -27,8 +27,9 @@ def main() -> None:
     ap.add_argument("--lookahead", default="learned", choices=["off", "filtered", "learned", "all"])
     ap.add_argument("--repeat", type=int, default=1)
     ap.add_argument("--graphs", action="store_true", help="resident engine: wave loop as a CUDA graph")
+    ap.add_argument("--replicas", type=int, default=1, help="configuration 3: exact replicas of the base rows")
     a = ap.parse_args()
-    kw = {"scale": a.scale} if a.cfg != 3 else {"scale": a.scale, "replicas": 1}
+    kw = {"scale": a.scale} if a.cfg != 3 else {"scale": a.scale, "replicas": a.replicas}
     db0 = synth.generate(a.cfg, **kw)
     minsup = a.minsup if a.minsup is not None else MINSUP[a.cfg]
     with Database.from_csr(db0.offsets, db0.items, minsup) as db:
