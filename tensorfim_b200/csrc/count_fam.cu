@@ -46,22 +46,19 @@ namespace {
 constexpr int kFM = 128;                               // accumulator lanes (F columns)
 constexpr int kFXRows = 144;                           // expanded rows per K block
 constexpr int kFKBytes = 128;                          // bytes (= bits) per row per K block
-constexpr int kFKBlocks = 2;                           // K blocks per stage: 256 bits
-constexpr int kFBlockBytes = kFXRows * kFKBytes;       // 18 KiB (a multiple of 1024)
-constexpr int kFStageBytes = kFKBlocks * kFBlockBytes; // 36 KiB
+constexpr int kFMaxKBlocks = 8;                        // K blocks per stage: 2, 4 or 8 (1024 bits)
+constexpr int kFStageBytes = 2 * kFXRows * kFKBytes;   // 36 KiB: 2 K blocks of 144 rows, or more of fewer
 constexpr int kFStages = 4;
 constexpr int kFExpWarps = 8;
 constexpr int kFLoadWarp = 1 + kFExpWarps;             // warp 9
 constexpr int kFThreads = 32 * (2 + kFExpWarps);       // 320
-constexpr int kFStageWords = kFKBlocks * kFKBytes / 32;   // 8 words of 32 bits per row per stage
-constexpr int kFStageRaw = kFStageWords * 4;           // 32 raw bytes per row per stage
 constexpr int kFRawSlots = 3;
 constexpr int kFRawSlotBytes = 24 * 1024;              // one chunk of raw rows
 constexpr int kFMaxEntries = kFM + 2;                  // rows + up to two base sources
 constexpr int kFSmem = kFStages * kFStageBytes + kFRawSlots * kFRawSlotBytes + 1024;
 constexpr uint32_t kFTmemCols = 256;
 constexpr uint32_t kFSpin = 1u << 22;
-static_assert(kFRawSlotBytes / (kFMaxEntries * kFStageRaw) >= 1, "a chunk holds at least one stage");
+static_assert(kFRawSlotBytes / (kFMaxEntries * 2 * 16) >= 1, "a chunk holds at least one stage");
 
 __device__ int g_fam_status;   // 0 ok, 1 an mbarrier wait expired
 
@@ -217,11 +214,18 @@ __global__ void __launch_bounds__(kFThreads, 1) k_count_fam(CountArgs a_val, con
         const int b8 = s0 & ~7;
         const int ncov = s0 + t.nr - b8;
         const int N = (ncov + 15) & ~15;           // 16 .. 144
-        const int n_st = (t.w1 - t.w0) / kFStageWords;
+        // rows of a K block (a multiple of 8, so K blocks stay 1024-byte aligned) and K blocks
+        // per stage: a narrow family takes more K per synchronisation
+        const int rows_alloc = max((nF + 7) & ~7, b8 + N);   // <= 144
+        const int KB = rows_alloc * kFKBytes * 8 <= kFStageBytes ? 8 : rows_alloc * kFKBytes * 4 <= kFStageBytes ? 4 : 2;
+        const uint32_t kb_bytes = (uint32_t)rows_alloc * kFKBytes;
+        const int stage_words = KB * 4;            // raw 32-bit words per row per stage
+        const int stage_raw = stage_words * 4;     // raw bytes per row per stage
+        const int n_st = (t.w1 - t.w0) / stage_words;
         const int nbase = (j.base_slot >= 0 ? 1 : 0) + (j.base_item >= 0 ? 1 : 0);
         const int n_ent = nF + nbase;
         // stages per raw chunk: a chunk of every entry fits one ring slot
-        const int C = max(1, kFRawSlotBytes / (n_ent * kFStageRaw));
+        const int C = max(1, kFRawSlotBytes / (n_ent * stage_raw));
         const int n_chunks = (n_st + C - 1) / C;
         // the tile's raw sources
         for (int q = tid; q < n_ent; q += kFThreads) {
@@ -246,9 +250,8 @@ __global__ void __launch_bounds__(kFThreads, 1) k_count_fam(CountArgs a_val, con
                     }
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                     const uint32_t stage = base + (uint32_t)s * kFStageBytes;
-#pragma unroll
-                    for (int kb = 0; kb < kFKBlocks; kb++) {
-                        const uint32_t blk = stage + (uint32_t)kb * kFBlockBytes;
+                    for (int kb = 0; kb < KB; kb++) {
+                        const uint32_t blk = stage + (uint32_t)kb * kb_bytes;
 #pragma unroll
                         for (int k = 0; k < kFKBytes / 32; k++) {
                             const uint64_t da = smem_desc(blk + k * 32);
@@ -276,31 +279,30 @@ __global__ void __launch_bounds__(kFThreads, 1) k_count_fam(CountArgs a_val, con
                 ok = __all_sync(0xffffffffu, ok);
                 if (!ok) break;
                 const int st0 = k * C, ns = min(C, n_st - st0);
-                const uint32_t bytes = (uint32_t)ns * kFStageRaw;   // per entry, a multiple of 32
+                const uint32_t bytes = (uint32_t)(ns * stage_raw);   // per entry, a multiple of 32
                 const uint32_t bar = smem_u32(&sh.rfull[slot]);
                 if (lane == 0) mbar_expect_tx(bar, bytes * (uint32_t)n_ent);
                 __syncwarp();
                 const uint32_t dst0 = raw_base + (uint32_t)slot * kFRawSlotBytes;
-                const int64_t w = t.w0 + (int64_t)st0 * kFStageWords;
+                const int64_t w = t.w0 + (int64_t)st0 * stage_words;
                 for (int q = lane; q < n_ent; q += 32)
-                    bulk_load(dst0 + (uint32_t)(q * C * kFStageRaw), sh.src[q] + w, bytes, bar);
+                    bulk_load(dst0 + (uint32_t)(q * C * stage_raw), sh.src[q] + w, bytes, bar);
             }
             if (!ok && lane == 0) {
                 atomicExch(&sh.abort, 1);
                 atomicExch(&g_fam_status, 1);
             }
         } else {
-            // ---- expansion: X rows r = e, e + 8, ... (< nF)
+            // ---- expansion: X rows r = e, e + 8, ... (< nF); a task is one 16-byte output chunk
+            // (row, K block, chunk c): 8 chunks per K block, KB * 8 per row
             const int e = warp - 1;
             const int nrw = nF > e ? (nF - e + kFExpWarps - 1) / kFExpWarps : 0;
+            const int tpr_log = KB == 8 ? 6 : KB == 4 ? 5 : 4;   // log2(KB * 8)
+            const int ntask = nrw << tpr_log;
+            const uint32_t ent = (uint32_t)(C * stage_raw);
             bool ok = true;
-            // lane -> (row of the pass, 16-byte output chunk): 2 rows per pass, 16 chunks per row
-            const int half = lane >> 4, chunk = lane & 15;
-            const int kb = chunk >> 3, c = chunk & 7;
-            const int qw = kb * 4 + (c >> 1);   // input word of this chunk within the stage
-            const int sh0 = 4 * (c & 1);
+            int k = 0, within = 0;   // chunk of the tile and stage within it
             for (int st = 0; st < n_st; st++) {
-                const int k = st / C, within = st - k * C;
                 const uint32_t ck = gc + (uint32_t)k;
                 const int slot = (int)(ck % kFRawSlots);
                 if (within == 0 && ok) ok = mbar_wait(smem_u32(&sh.rfull[slot]), (ck / kFRawSlots) & 1u);
@@ -310,33 +312,35 @@ __global__ void __launch_bounds__(kFThreads, 1) k_count_fam(CountArgs a_val, con
                     ok = mbar_wait(smem_u32(&sh.empty[s]), ((it / kFStages) - 1u) & 1u);
                 ok = __all_sync(0xffffffffu, ok);
                 if (!ok) break;
-                // raw word qw of entry q at stage `within` of the slot
-                const uint32_t rs = raw_base + (uint32_t)slot * kFRawSlotBytes + (uint32_t)(within * kFStageRaw + qw * 4);
-                const uint32_t ent = (uint32_t)(C * kFStageRaw);
-                uint32_t bw = ~0u;
-                for (int b = 0; b < nbase; b++) {
+                const uint32_t rs = raw_base + (uint32_t)slot * kFRawSlotBytes + (uint32_t)(within * stage_raw);
+                const uint32_t stage = base + (uint32_t)s * kFStageBytes;
+                for (int tk = lane; tk < ntask; tk += 32) {
+                    const int qi = tk >> tpr_log, rem = tk & ((1 << tpr_log) - 1);
+                    const int kb = rem >> 3, c = rem & 7;
+                    const uint32_t off = (uint32_t)((kb * 4 + (c >> 1)) * 4);   // raw word of the chunk
+                    const int r = e + qi * kFExpWarps;
                     uint32_t x;
-                    asm volatile("ld.shared.b32 %0, [%1];" : "=r"(x) : "r"(rs + (uint32_t)(nF + b) * ent));
-                    bw &= x;
-                }
-                const uint32_t stage = base + (uint32_t)s * kFStageBytes + (uint32_t)kb * kFBlockBytes;
-                for (int q0 = 0; q0 < nrw; q0 += 2) {
-                    const int q = q0 + half;
-                    if (q < nrw) {
-                        const int r = e + q * kFExpWarps;
-                        uint32_t x;
-                        asm volatile("ld.shared.b32 %0, [%1];" : "=r"(x) : "r"(rs + (uint32_t)r * ent));
-                        x = (x & bw) >> sh0;
-                        st_shared_v4(stage + (uint32_t)r * kFKBytes + (uint32_t)((c ^ (r & 7)) << 4), x & 0x01010101u,
-                                     (x >> 1) & 0x01010101u, (x >> 2) & 0x01010101u, (x >> 3) & 0x01010101u);
+                    asm volatile("ld.shared.b32 %0, [%1];" : "=r"(x) : "r"(rs + (uint32_t)r * ent + off));
+                    for (int b = 0; b < nbase; b++) {
+                        uint32_t y;
+                        asm volatile("ld.shared.b32 %0, [%1];" : "=r"(y) : "r"(rs + (uint32_t)(nF + b) * ent + off));
+                        x &= y;
                     }
+                    x >>= 4 * (c & 1);
+                    st_shared_v4(stage + (uint32_t)kb * kb_bytes + (uint32_t)r * kFKBytes + (uint32_t)((c ^ (r & 7)) << 4),
+                                 x & 0x01010101u, (x >> 1) & 0x01010101u, (x >> 2) & 0x01010101u, (x >> 3) & 0x01010101u);
                 }
                 // generic-proxy stores -> visible to the tensor cores' async proxy
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 __syncwarp();
+                const bool chunk_end = within == C - 1 || st == n_st - 1;
                 if (lane == 0) {
                     mbar_arrive(smem_u32(&sh.full[s]));
-                    if (within == C - 1 || st == n_st - 1) mbar_arrive(smem_u32(&sh.rempty[slot]));
+                    if (chunk_end) mbar_arrive(smem_u32(&sh.rempty[slot]));
+                }
+                if (++within == C) {
+                    within = 0;
+                    k++;
                 }
             }
             if (!ok && lane == 0) {
