@@ -16,24 +16,22 @@
 // s0 & ~7 (8-row groups keep the 128-byte swizzle phase) and spans N = roundup16 of what
 // it must cover, at most 144 rows, so the expanded stage holds 144 rows.
 //
-// Warp roles (320 threads, one CTA per SM, persistent over a tile counter):
-//   warp 0     : one lane issues the stage's 8 MMAs (K = 32 bytes each, 2 K blocks of
-//                128 bits) once the stage is full, and commits them to the stage's `empty`
-//                barrier; after the tile's last stage it commits to `done`;
-//   warp 9     : the loader: the raw bit words of a chunk of stages -- every X row's item
-//                row and the base's one or two sources, C stages of 256 bits each -- come
-//                into a three-slot ring with one bulk copy (cp.async.bulk, the TMA engine's
-//                untiled copy of this GPU's own memory) per row and chunk, completing on
-//                the slot's transaction-count barrier.  A chunk is about 24 KiB whatever
-//                the family's width (C = 5 stages at 130 rows, 42 at 18), so about 72 KiB
-//                are in flight per SM;
-//   warps 1..8 : X rows r = warp-1 (mod 8): the stage's raw words, ANDed with the base, are
-//                expanded (byte lane b of output word 8q+i is bit i+8b of input word q; any K
-//                order shared by both operands works) and stored in the K-major
-//                128-byte-swizzle layout; each warp arrives on the stage's `full` barrier and,
-//                after a chunk's last stage, on the slot's `rempty` barrier; warps 1..4 then
-//                read the accumulator (tcgen05.ld, 32 lanes each) and add the counts to the
-//                job's output with int32 atomics (word slices of one job meet there).
+// Warp roles (288 threads, one CTA per SM, persistent over a tile counter):
+//   warp 0     : one lane issues the stage's MMAs (K = 32 bytes each, 4 per K block of 128
+//                bits, 2, 4 or 8 K blocks per stage by the family's width) once the stage is
+//                full, and commits them to the stage's `empty` barrier; after the tile's last
+//                stage it commits to `done`;
+//   warps 1..8 : each lane owns one (X row, K block) unit of its warp's rows r = warp-1
+//                (mod 8): it loads the unit's 128 raw bits and the base's with 16-byte
+//                read-only loads four stages ahead into registers, ANDs them, expands them
+//                (byte lane b of output word 8q+i is bit i+8b of input word q; any K order
+//                shared by both operands works) into the K-major 128-byte-swizzle layout,
+//                and the warp arrives on the stage's `full` barrier; warps 1..4 then read the
+//                accumulator (tcgen05.ld, 32 lanes each) and add the counts to the job's output
+//                with int32 atomics (word slices of one job meet there).
+// The tensor core issues an i8 MMA of M = 128 in about 50 cycles up to N = 64 (64 at N = 128,
+// 128 at N = 256), so this counter pays for families wide enough to fill it; narrow ones
+// stay on the CUDA-core tiles.
 // Every mbarrier wait is bounded; on expiry the kernel records an error, stops issuing,
 // drains what it issued and frees its tensor memory.
 #include <atomic>
@@ -46,19 +44,14 @@ namespace {
 constexpr int kFM = 128;                               // accumulator lanes (F columns)
 constexpr int kFXRows = 144;                           // expanded rows per K block
 constexpr int kFKBytes = 128;                          // bytes (= bits) per row per K block
-constexpr int kFMaxKBlocks = 8;                        // K blocks per stage: 2, 4 or 8 (1024 bits)
 constexpr int kFStageBytes = 2 * kFXRows * kFKBytes;   // 36 KiB: 2 K blocks of 144 rows, or more of fewer
-constexpr int kFStages = 4;
+constexpr int kFStages = 6;
 constexpr int kFExpWarps = 8;
-constexpr int kFLoadWarp = 1 + kFExpWarps;             // warp 9
-constexpr int kFThreads = 32 * (2 + kFExpWarps);       // 320
-constexpr int kFRawSlots = 3;
-constexpr int kFRawSlotBytes = 24 * 1024;              // one chunk of raw rows
-constexpr int kFMaxEntries = kFM + 2;                  // rows + up to two base sources
-constexpr int kFSmem = kFStages * kFStageBytes + kFRawSlots * kFRawSlotBytes + 1024;
+constexpr int kFThreads = 32 * (1 + kFExpWarps);       // 288
+constexpr int kFAhead = 4;                             // stages of raw words in flight per lane
+constexpr int kFSmem = kFStages * kFStageBytes + 1024;
 constexpr uint32_t kFTmemCols = 256;
 constexpr uint32_t kFSpin = 1u << 22;
-static_assert(kFRawSlotBytes / (kFMaxEntries * 2 * 16) >= 1, "a chunk holds at least one stage");
 
 __device__ int g_fam_status;   // 0 ok, 1 an mbarrier wait expired
 
@@ -68,17 +61,7 @@ __device__ __forceinline__ void st_shared_v4(uint32_t addr, uint32_t a, uint32_t
     asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(a), "r"(b), "r"(c), "r"(d) : "memory");
 }
 
-// Bulk copy of `bytes` (a multiple of 16, both addresses 16-byte aligned) from this GPU's
-// global memory into shared memory, completing on the barrier's transaction count.
-__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-                 "l"(src), "r"(bytes), "r"(bar)
-                 : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
-    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(bar), "r"(bytes)
-                 : "memory");
-}
+__device__ __forceinline__ uint4 ldg4(const uint32_t* p) { return __ldg(reinterpret_cast<const uint4*>(p)); }
 
 // K-major, 128-byte swizzle shared-memory matrix descriptor: start address, leading byte
 // offset 16 (unused by swizzled K-major layouts), stride byte offset 1024 (8-row groups),
@@ -148,10 +131,9 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
 }
 
 struct FamShared {
-    uint64_t full[kFStages], empty[kFStages], done, rfull[kFRawSlots], rempty[kFRawSlots];
+    uint64_t full[kFStages], empty[kFStages], done;
     uint32_t tmem;
     int32_t tile, abort;
-    const uint32_t* src[kFMaxEntries];   // raw sources of the tile: X rows, then the base's
 };
 
 // a_dev (device copy of the arguments, read when non-null: a graph's launches outlive pool
@@ -164,7 +146,6 @@ __global__ void __launch_bounds__(kFThreads, 1) k_count_fam(CountArgs a_val, con
     const CountArgs a = a_dev ? *a_dev : a_val;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t base = (smem_u32(smem_raw) + 1023u) & ~1023u;
-    const uint32_t raw_base = base + kFStages * kFStageBytes;
     const int32_t n_tiles = n_tiles_p ? *n_tiles_p : n_tiles_h;
     const int64_t W = a.W;
 
@@ -173,10 +154,6 @@ __global__ void __launch_bounds__(kFThreads, 1) k_count_fam(CountArgs a_val, con
         for (int s = 0; s < kFStages; s++) {
             mbar_init(smem_u32(&sh.full[s]), kFExpWarps);
             mbar_init(smem_u32(&sh.empty[s]), 1);
-        }
-        for (int s = 0; s < kFRawSlots; s++) {
-            mbar_init(smem_u32(&sh.rfull[s]), 1);
-            mbar_init(smem_u32(&sh.rempty[s]), kFExpWarps);
         }
         mbar_init(smem_u32(&sh.done), 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -193,7 +170,6 @@ __global__ void __launch_bounds__(kFThreads, 1) k_count_fam(CountArgs a_val, con
     const uint32_t tmem = sh.tmem;
 
     uint32_t g = 0;        // stages of the CTA before the current tile (phases of full / empty)
-    uint32_t gc = 0;       // raw chunks of the CTA before the current tile (phases of rfull / rempty)
     uint32_t n_done = 0;   // tiles finished (phase of `done`)
     bool first = true;
     while (true) {
@@ -215,27 +191,14 @@ __global__ void __launch_bounds__(kFThreads, 1) k_count_fam(CountArgs a_val, con
         const int ncov = s0 + t.nr - b8;
         const int N = (ncov + 15) & ~15;           // 16 .. 144
         // rows of a K block (a multiple of 8, so K blocks stay 1024-byte aligned) and K blocks
-        // per stage: a narrow family takes more K per synchronisation
-        const int rows_alloc = max((nF + 7) & ~7, b8 + N);   // <= 144
-        const int KB = rows_alloc * kFKBytes * 8 <= kFStageBytes ? 8 : rows_alloc * kFKBytes * 4 <= kFStageBytes ? 4 : 2;
+        // per stage: a narrow family takes more K per synchronisation; a warp's units (rows x
+        // K blocks) never exceed its 32 lanes
+        const int rows_alloc = max((nF + 7) & ~7, b8 + N);   // <= 136
+        const int KB = (nF <= 32 && rows_alloc * kFKBytes * 8 <= kFStageBytes) ? 8
+                       : (nF <= 64 && rows_alloc * kFKBytes * 4 <= kFStageBytes) ? 4 : 2;
         const uint32_t kb_bytes = (uint32_t)rows_alloc * kFKBytes;
         const int stage_words = KB * 4;            // raw 32-bit words per row per stage
-        const int stage_raw = stage_words * 4;     // raw bytes per row per stage
         const int n_st = (t.w1 - t.w0) / stage_words;
-        const int nbase = (j.base_slot >= 0 ? 1 : 0) + (j.base_item >= 0 ? 1 : 0);
-        const int n_ent = nF + nbase;
-        // stages per raw chunk: a chunk of every entry fits one ring slot
-        const int C = max(1, kFRawSlotBytes / (n_ent * stage_raw));
-        const int n_chunks = (n_st + C - 1) / C;
-        // the tile's raw sources
-        for (int q = tid; q < n_ent; q += kFThreads) {
-            const uint32_t* p;
-            if (q < nF) p = a.bitmap + (int64_t)a.cols[j.col_off + q] * W;
-            else if (q == nF && j.base_slot >= 0) p = a.masks + (int64_t)j.base_slot * W;
-            else p = a.bitmap + (int64_t)j.base_item * W;
-            sh.src[q] = p;
-        }
-        __syncthreads();
 
         if (warp == 0) {
             if (lane == 0) {
@@ -269,78 +232,62 @@ __global__ void __launch_bounds__(kFThreads, 1) k_count_fam(CountArgs a_val, con
                 tc_commit(smem_u32(&sh.done));
             }
             __syncwarp();
-        } else if (warp == kFLoadWarp) {
-            // ---- loader: chunk k of the tile into slot (gc + k) % kFRawSlots
-            bool ok = true;
-            for (int k = 0; k < n_chunks; k++) {
-                const uint32_t ck = gc + (uint32_t)k;
-                const int slot = (int)(ck % kFRawSlots);
-                if (ck >= (uint32_t)kFRawSlots) ok = mbar_wait(smem_u32(&sh.rempty[slot]), ((ck / kFRawSlots) - 1u) & 1u);
-                ok = __all_sync(0xffffffffu, ok);
-                if (!ok) break;
-                const int st0 = k * C, ns = min(C, n_st - st0);
-                const uint32_t bytes = (uint32_t)(ns * stage_raw);   // per entry, a multiple of 32
-                const uint32_t bar = smem_u32(&sh.rfull[slot]);
-                if (lane == 0) mbar_expect_tx(bar, bytes * (uint32_t)n_ent);
-                __syncwarp();
-                const uint32_t dst0 = raw_base + (uint32_t)slot * kFRawSlotBytes;
-                const int64_t w = t.w0 + (int64_t)st0 * stage_words;
-                for (int q = lane; q < n_ent; q += 32)
-                    bulk_load(dst0 + (uint32_t)(q * C * stage_raw), sh.src[q] + w, bytes, bar);
-            }
-            if (!ok && lane == 0) {
-                atomicExch(&sh.abort, 1);
-                atomicExch(&g_fam_status, 1);
-            }
         } else {
-            // ---- expansion: X rows r = e, e + 8, ... (< nF); a task is one 16-byte output chunk
-            // (row, K block, chunk c): 8 chunks per K block, KB * 8 per row
+            // ---- expansion: lane -> unit (row q of the warp's rows, K block kb)
             const int e = warp - 1;
             const int nrw = nF > e ? (nF - e + kFExpWarps - 1) / kFExpWarps : 0;
-            const int tpr_log = KB == 8 ? 6 : KB == 4 ? 5 : 4;   // log2(KB * 8)
-            const int ntask = nrw << tpr_log;
-            const uint32_t ent = (uint32_t)(C * stage_raw);
+            const int kb_log = KB == 8 ? 3 : KB == 4 ? 2 : 1;
+            const bool active = lane < (nrw << kb_log);
+            const int q = lane >> kb_log, kb = lane & (KB - 1);
+            const int r = e + q * kFExpWarps;
+            const uint32_t* src = active ? a.bitmap + (int64_t)a.cols[j.col_off + r] * W : nullptr;
+            const uint32_t* bm = j.base_slot >= 0 ? a.masks + (int64_t)j.base_slot * W : nullptr;
+            const uint32_t* bi = j.base_item >= 0 ? a.bitmap + (int64_t)j.base_item * W : nullptr;
+            const int64_t w_unit = t.w0 + (int64_t)kb * 4;   // + st * stage_words
+            const uint4 ones = make_uint4(~0u, ~0u, ~0u, ~0u);
+            uint4 pr[kFAhead], pm[kFAhead], pi[kFAhead];
+            auto load = [&](int st, uint4& xr, uint4& xm, uint4& xi) {
+                xr = xm = xi = ones;
+                if (active && st < n_st) {
+                    const int64_t w = w_unit + (int64_t)st * stage_words;
+                    xr = ldg4(src + w);
+                    if (bm) xm = ldg4(bm + w);
+                    if (bi) xi = ldg4(bi + w);
+                }
+            };
+#pragma unroll
+            for (int d = 0; d < kFAhead; d++) load(d, pr[d], pm[d], pi[d]);
+            const uint32_t row_off = (uint32_t)r * kFKBytes + (uint32_t)kb * kb_bytes;
+            const int rs = r & 7;
             bool ok = true;
-            int k = 0, within = 0;   // chunk of the tile and stage within it
-            for (int st = 0; st < n_st; st++) {
-                const uint32_t ck = gc + (uint32_t)k;
-                const int slot = (int)(ck % kFRawSlots);
-                if (within == 0 && ok) ok = mbar_wait(smem_u32(&sh.rfull[slot]), (ck / kFRawSlots) & 1u);
-                const uint32_t it = g + (uint32_t)st;
-                const int s = (int)(it % kFStages);
-                if (ok && it >= (uint32_t)kFStages)
-                    ok = mbar_wait(smem_u32(&sh.empty[s]), ((it / kFStages) - 1u) & 1u);
-                ok = __all_sync(0xffffffffu, ok);
-                if (!ok) break;
-                const uint32_t rs = raw_base + (uint32_t)slot * kFRawSlotBytes + (uint32_t)(within * stage_raw);
-                const uint32_t stage = base + (uint32_t)s * kFStageBytes;
-                for (int tk = lane; tk < ntask; tk += 32) {
-                    const int qi = tk >> tpr_log, rem = tk & ((1 << tpr_log) - 1);
-                    const int kb = rem >> 3, c = rem & 7;
-                    const uint32_t off = (uint32_t)((kb * 4 + (c >> 1)) * 4);   // raw word of the chunk
-                    const int r = e + qi * kFExpWarps;
-                    uint32_t x;
-                    asm volatile("ld.shared.b32 %0, [%1];" : "=r"(x) : "r"(rs + (uint32_t)r * ent + off));
-                    for (int b = 0; b < nbase; b++) {
-                        uint32_t y;
-                        asm volatile("ld.shared.b32 %0, [%1];" : "=r"(y) : "r"(rs + (uint32_t)(nF + b) * ent + off));
-                        x &= y;
+            for (int st0 = 0; st0 < n_st && ok; st0 += kFAhead) {
+#pragma unroll
+                for (int d = 0; d < kFAhead; d++) {
+                    const int st = st0 + d;
+                    if (st >= n_st) break;
+                    const uint32_t it = g + (uint32_t)st;
+                    const int s = (int)(it % kFStages);
+                    if (ok && it >= (uint32_t)kFStages)
+                        ok = mbar_wait(smem_u32(&sh.empty[s]), ((it / kFStages) - 1u) & 1u);
+                    ok = __all_sync(0xffffffffu, ok);
+                    if (!ok) break;
+                    const uint4 x = make_uint4(pr[d].x & pm[d].x & pi[d].x, pr[d].y & pm[d].y & pi[d].y,
+                                               pr[d].z & pm[d].z & pi[d].z, pr[d].w & pm[d].w & pi[d].w);
+                    load(st + kFAhead, pr[d], pm[d], pi[d]);
+                    if (active) {
+                        const uint32_t row = base + (uint32_t)s * kFStageBytes + row_off;
+                        const uint32_t ws[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+                        for (int c = 0; c < 8; c++) {
+                            const uint32_t v = ws[c >> 1] >> (4 * (c & 1));
+                            st_shared_v4(row + (uint32_t)((c ^ rs) << 4), v & 0x01010101u, (v >> 1) & 0x01010101u,
+                                         (v >> 2) & 0x01010101u, (v >> 3) & 0x01010101u);
+                        }
                     }
-                    x >>= 4 * (c & 1);
-                    st_shared_v4(stage + (uint32_t)kb * kb_bytes + (uint32_t)r * kFKBytes + (uint32_t)((c ^ (r & 7)) << 4),
-                                 x & 0x01010101u, (x >> 1) & 0x01010101u, (x >> 2) & 0x01010101u, (x >> 3) & 0x01010101u);
-                }
-                // generic-proxy stores -> visible to the tensor cores' async proxy
-                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                __syncwarp();
-                const bool chunk_end = within == C - 1 || st == n_st - 1;
-                if (lane == 0) {
-                    mbar_arrive(smem_u32(&sh.full[s]));
-                    if (chunk_end) mbar_arrive(smem_u32(&sh.rempty[slot]));
-                }
-                if (++within == C) {
-                    within = 0;
-                    k++;
+                    // generic-proxy stores -> visible to the tensor cores' async proxy
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(smem_u32(&sh.full[s]));
                 }
             }
             if (!ok && lane == 0) {
@@ -377,10 +324,9 @@ __global__ void __launch_bounds__(kFThreads, 1) k_count_fam(CountArgs a_val, con
             }
         }
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        __syncthreads();   // accumulator read, stages, ring and tables free for the next tile
+        __syncthreads();   // accumulator read, stages free for the next tile
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         g += (uint32_t)max(n_st, 0);
-        gc += (uint32_t)n_chunks;
         n_done++;
     }
     __syncthreads();
