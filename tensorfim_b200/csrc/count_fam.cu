@@ -45,11 +45,17 @@ constexpr int kFM = 128;                               // accumulator lanes (F c
 constexpr int kFXRows = 144;                           // expanded rows per K block
 constexpr int kFKBytes = 128;                          // bytes (= bits) per row per K block
 constexpr int kFStageBytes = 2 * kFXRows * kFKBytes;   // 36 KiB: 2 K blocks of 144 rows, or more of fewer
-constexpr int kFStages = 6;
+constexpr int kFStages = 5;
 constexpr int kFExpWarps = 8;
 constexpr int kFThreads = 32 * (1 + kFExpWarps);       // 288
 constexpr int kFAhead = 4;                             // stages of raw words in flight per lane
-constexpr int kFSmem = kFStages * kFStageBytes + 1024;
+// The A operand (M = 128 rows of 128 bytes) of a K block spans 16 KiB from the block's start
+// whatever the family's width; when a K block holds fewer than 128 rows the window runs into
+// the following blocks (rows the epilogue discards), so a guard of 16 KiB follows the last
+// stage to keep every window inside the allocation.
+constexpr int kFGuard = kFM * kFKBytes;
+constexpr int kFSmem = kFStages * kFStageBytes + kFGuard + 1024;
+static_assert(kFSmem <= 227 * 1024 - 256, "stages + guard + alignment fit the opt-in shared memory");
 constexpr uint32_t kFTmemCols = 256;
 constexpr uint32_t kFSpin = 1u << 22;
 
@@ -196,6 +202,8 @@ __global__ void __launch_bounds__(kFThreads, 1) k_count_fam(CountArgs a_val, con
         const int rows_alloc = max((nF + 7) & ~7, b8 + N);   // <= 136
         const int KB = (nF <= 32 && rows_alloc * kFKBytes * 8 <= kFStageBytes) ? 8
                        : (nF <= 64 && rows_alloc * kFKBytes * 4 <= kFStageBytes) ? 4 : 2;
+        // the last A window of a stage, (KB - 1) * kb_bytes + 16 KiB from the stage, stays
+        // inside stage + guard: KB * kb_bytes <= kFStageBytes and the guard is 16 KiB
         const uint32_t kb_bytes = (uint32_t)rows_alloc * kFKBytes;
         const int stage_words = KB * 4;            // raw 32-bit words per row per stage
         const int n_st = (t.w1 - t.w0) / stage_words;

@@ -194,3 +194,38 @@ def test_path_rooflines_arithmetic():
     assert abs(p["lop3"]["share_of_counting"] - 2 / 3) < 1e-12
     r = measure.headline_roofline(p, 6000.0, 1e15, "measured", "measured")
     assert r["kernel"] == "k_count_lop3" and r["bound"] == "hbm" and abs(r["frac"] - 1 / 3) < 1e-12
+
+
+def test_family_counter_shared_memory_windows():
+    """The tcgen05 family counter's shared-memory layout (csrc/count_fam.cu), restated: for
+    every tile the pack can emit (nF <= 128 columns, rows a run [s0, s0 + nr) of them), every
+    expanded row, every A window (128 rows from a K block's start) and every B window stays
+    inside the allocation, K blocks are 1024-byte aligned and a warp's units fit its lanes."""
+    stage_bytes, stages, guard, kbytes, align = 2 * 144 * 128, 5, 128 * 128, 128, 1024
+    smem = stages * stage_bytes + guard + align
+    assert smem <= 227 * 1024 - 256
+    worst = 0
+    for nF in range(1, 129):
+        for s0 in range(0, nF):
+            for nr in range(1, nF - s0 + 1):
+                b8 = s0 & ~7
+                N = (s0 + nr - b8 + 15) & ~15
+                assert 16 <= N <= 144 and N % 16 == 0
+                rows_alloc = max((nF + 7) & ~7, b8 + N)
+                assert rows_alloc % 8 == 0 and rows_alloc <= 136
+                if nF <= 32 and rows_alloc * kbytes * 8 <= stage_bytes:
+                    KB = 8
+                elif nF <= 64 and rows_alloc * kbytes * 4 <= stage_bytes:
+                    KB = 4
+                else:
+                    KB = 2
+                kb_bytes = rows_alloc * kbytes
+                assert kb_bytes % 1024 == 0 and KB * kb_bytes <= stage_bytes
+                nrw = (nF + 7) // 8
+                assert nrw * KB <= 32
+                last = (stages - 1) * stage_bytes + (KB - 1) * kb_bytes
+                a_end = last + 128 * kbytes
+                b_end = last + (b8 + N) * kbytes
+                worst = max(worst, a_end, b_end)
+    # the aligned base lies at most align - 1 bytes into the allocation
+    assert worst + align - 1 <= smem
