@@ -287,6 +287,7 @@ typedef struct {
 #define TFIM_PATH_TC     2   /* tcgen05.mma kind::i8 tiles (bits expanded to bytes) */
 #define TFIM_PATH_PAIRS  3   /* pair co-occurrence over the reduced transaction list */
 #define TFIM_PATH_PROJ   4   /* projected counting over the prefix's transactions */
+#define TFIM_PATH_GRAM   5   /* register-tiled AND+popc Gram blocks of dense narrow families */
 
 /* ------------------------------------------------------------------ tuning table
  * Launch shapes and counter selection of the engines.  The reference fixes these as

@@ -119,7 +119,7 @@ class MineStats(C.Structure):
 
 
 # counting paths of MineStats.path_* (include/tfim.h TFIM_PATH_*)
-PATHS = ["lop3", "b1", "tc", "pairs", "proj"]
+PATHS = ["lop3", "b1", "tc", "pairs", "proj", "gram"]
 
 
 _lib = None

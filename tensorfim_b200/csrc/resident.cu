@@ -57,11 +57,12 @@ struct DJob {
     int32_t b3l, heavy;        // CUDA-core tiles: heavy jobs' tiles come first (prefix b3), then the light
                                // jobs' (prefix b3l after all heavy tiles)
     int32_t btc;               // exclusive prefix of the tcgen05 family counter's jobs
+    int32_t bgr;               // exclusive prefix of the CUDA-core Gram counter's jobs
 };
 
 // Phases of a wave (device-time stamps) and counter classes of a count job.
-enum { kPhPack = 0, kPhZero, kPhLop3, kPhB1, kPhTc, kPhProj, kPhExpand, kPhMasks, kPhases };
-enum { kClsLop3 = 0, kClsB1 = 1, kClsProj = 2, kClsTc = 3, kClasses = 4 };
+enum { kPhPack = 0, kPhZero, kPhLop3, kPhB1, kPhTc, kPhProj, kPhGram, kPhExpand, kPhMasks, kPhases };
+enum { kClsLop3 = 0, kClsB1 = 1, kClsProj = 2, kClsTc = 3, kClsGram = 4, kClasses = 5 };
 
 struct ResStatus {
     int32_t stack_n, look_n, fam_n, item_n, head_n, mfi_n, mfi_item_n, slot_n, free_n, free_taken, defer_n, log_n;
@@ -74,6 +75,7 @@ struct ResStatus {
     int64_t g_out, g_tiles;
     int32_t launch_id, next3, next1, pad1;   // next3 / next1: tile counters of the persistent counters
     int32_t tiles_tc, next_tc;               // tcgen05 family counter: tiles, tile counter
+    int32_t tiles_gr, next_gr;               // CUDA-core Gram counter: tiles, tile counter
     unsigned long long launch_t0;
     unsigned long long supports, nodes, lookaheads, hits, skipped, pep;
     // superset check: MFIs [0, sup_done) are in the item -> MFI index the expand reads
@@ -125,6 +127,7 @@ struct ResPtrs {
     TileDesc* tiles_l3;
     TileDesc* tiles_b1;
     TileDesc* tiles_tc;
+    TileDesc* tiles_gr;
     int32_t* counts;
     // constants
     const uint32_t* bitmap;
@@ -179,7 +182,7 @@ __host__ __device__ __forceinline__ int column_block(int nF) { return max(128, (
 // only rewrites this record (the captured launches stay valid).
 struct ResArgs {
     ResPtrs p;
-    CountArgs a3, a1, ap, atc;   // CUDA-core, b1, projected and tcgen05 family counters
+    CountArgs a3, a1, ap, atc, agr;   // CUDA-core, b1, projected, tcgen05 family and Gram counters
 };
 
 __device__ __forceinline__ unsigned long long globaltimer() { return dev_globaltimer(); }
@@ -217,6 +220,17 @@ __device__ __forceinline__ bool use_tc(const ResPtrs& p, const JobDesc& jd, int3
     return d >= p.tc_min_density;
 }
 
+// The CUDA-core Gram counter takes a dense family job of at most kGramMaxCols columns (and at
+// most 128 blocks of 4 x 4 pairs) that the tensor counter does not: a dense prefix has no zero
+// word for the general tiles to skip, so the register-tiled Gram block is faster.
+__device__ __forceinline__ bool use_gram(const ResPtrs& p, const JobDesc& jd, int32_t sup) {
+    if (jd.n_cols < 1 || jd.n_cols > kGramMaxCols || jd.n_rows < 1) return false;
+    if (((jd.n_rows + 3) / 4) * ((jd.n_cols + 3) / 4) > 128) return false;
+    if (p.counter != TFIM_COUNTER_AUTO) return false;
+    const float d = p.n_bits > 0 ? fminf(1.f, 128.f * (float)sup / (float)p.n_bits) : 1.f;
+    return d >= p.tc_min_density;
+}
+
 __device__ __forceinline__ bool use_b1_shape(const ResPtrs& p, int nr, int nc) {
     if (p.counter == TFIM_COUNTER_LOP3) return false;
     if (p.counter == TFIM_COUNTER_TENSOR) return true;
@@ -247,7 +261,7 @@ __device__ __forceinline__ int find_job_by_tile(const DJob* dj, int nj, int64_t 
     int lo = 0, hi = nj - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
-        const int32_t v = K == 0 ? dj[mid].b3 : K == 1 ? dj[mid].b1 : K == 2 ? dj[mid].b3l : dj[mid].btc;
+        const int32_t v = K == 0 ? dj[mid].b3 : K == 1 ? dj[mid].b1 : K == 2 ? dj[mid].b3l : K == 3 ? dj[mid].btc : dj[mid].bgr;
         if (v <= t) lo = mid; else hi = mid - 1;
     }
     return lo;
@@ -322,7 +336,7 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
             const DFam f = p.fams[L.fam];
             DJob dj;
             dj.fam = L.fam; dj.kind = kJobLook; dj.r0 = 0; dj.nr = 1; dj.slot = L.slot; dj.log = L.log; dj.b3 = 0; dj.b1 = 0;
-            dj.cls = 0; dj.sl3 = 1; dj.b3l = 0; dj.heavy = 0; dj.btc = 0;
+            dj.cls = 0; dj.sl3 = 1; dj.b3l = 0; dj.heavy = 0; dj.btc = 0; dj.bgr = 0;
             p.djobs[k] = dj;
             JobDesc jd;
             jd.base_slot = -1; jd.base_item = -1; jd.n_rows = 1; jd.n_cols = f.nF - f.nT + 1;
@@ -426,7 +440,7 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
             const int32_t jid = s_n_jobs + (int32_t)hx[q];
             DJob dj;
             dj.fam = fid; dj.kind = kJobFam; dj.r0 = f.next_row; dj.nr = take[q]; dj.slot = -1; dj.log = -1; dj.b3 = 0; dj.b1 = 0;
-            dj.cls = 0; dj.sl3 = 1; dj.b3l = 0; dj.heavy = 0; dj.btc = 0;
+            dj.cls = 0; dj.sl3 = 1; dj.b3l = 0; dj.heavy = 0; dj.btc = 0; dj.bgr = 0;
             p.djobs[jid] = dj;
             JobDesc jd;
             jd.base_slot = f.slot; jd.base_item = f.item; jd.n_rows = take[q]; jd.n_cols = f.nF;
@@ -482,13 +496,14 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
         return P4 * (1.f + d * (2.f + nr + nr * nc / 32.f));
     };
     float cost_local = 0.f;
-    int64_t tot1 = 0, tottc = 0;
+    int64_t tot1 = 0, tottc = 0, totgr = 0;
     for (int base = 0; base < nj; base += kPackCand) {
-        int64_t a1[kPackItems], x1[kPackItems], at[kPackItems], xt[kPackItems];
+        int64_t a1[kPackItems], x1[kPackItems], at[kPackItems], xt[kPackItems], ag[kPackItems], xg[kPackItems];
         for (int q = 0; q < kPackItems; q++) {
             const int j = base + tid * kPackItems + q;
             a1[q] = 0;
             at[q] = 0;
+            ag[q] = 0;
             if (j < nj) {
                 const JobDesc jd = p.jobs[j];
                 DJob* djp = p.djobs + j;
@@ -502,6 +517,9 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
                 } else if (fam && use_tc(p, jd, fsup)) {
                     cls = kClsTc;
                     at[q] = 1;
+                } else if (fam && use_gram(p, jd, fsup)) {
+                    cls = kClsGram;
+                    ag[q] = 1;
                 } else if (use_b1_shape(p, jd.n_rows, jd.n_cols) && fam) {
                     cls = kClsB1;
                     a1[q] = b1_tiles(jd.n_rows, jd.n_cols);
@@ -517,15 +535,20 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
         Scan(tmp.scan).ExclusiveSum(at, xt, s_agg);
         __syncthreads();
         const int64_t gt = s_agg;
+        Scan(tmp.scan).ExclusiveSum(ag, xg, s_agg);
+        __syncthreads();
+        const int64_t gg = s_agg;
         for (int q = 0; q < kPackItems; q++) {
             const int j = base + tid * kPackItems + q;
             if (j < nj) {
                 p.djobs[j].b1 = (int32_t)(tot1 + x1[q]);
                 p.djobs[j].btc = (int32_t)(tottc + xt[q]);
+                p.djobs[j].bgr = (int32_t)(totgr + xg[q]);
             }
         }
         tot1 += g1;
         tottc += gt;
+        totgr += gg;
         __syncthreads();
     }
     __shared__ float s_cost;
@@ -595,9 +618,18 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
     if (wsltc <= 0) wsltc = 64;
     const int64_t ntc = W > 0 ? (W + wsltc - 1) / wsltc : 1;
     const int64_t TT = tottc * ntc;
+    // CUDA-core Gram tiles: every job whole, over `slgr` word slices (multiples of 64 words)
+    const int64_t want_gr = lmax(1, (int64_t)(p.l3_slices_per_sm * (float)p.sm_count));
+    int64_t slgr = totgr > 0 ? lmax(1, (want_gr + totgr - 1) / totgr) : 1;
+    slgr = lmin(slgr, lmax(1, W / 64));
+    int64_t wslgr = ((W / 64 + slgr - 1) / slgr) * 64;
+    if (wslgr <= 0) wslgr = 64;
+    const int64_t ngr = W > 0 ? (W + wslgr - 1) / wslgr : 1;
+    const int64_t TG = totgr * ngr;
     // the wave is committed only when the worst case of its expand fits the pools
     if (tid == 0) {
         const bool fit = s_out_total <= p.cap_out && T1 <= p.cap_tiles && T3 <= p.cap_tiles && TT <= p.cap_tiles &&
+                         TG <= p.cap_tiles &&
                          wave_fits(p.caps, *st, rows_total, nj, s_out_total, s_max_head, s_max_cols, p.log_on != 0);
         s_fit = fit;
         if (!fit) {
@@ -607,13 +639,13 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
             st->g_out = s_out_total;
             st->g_max_head = s_max_head;
             st->g_max_cols = s_max_cols;
-            st->g_tiles = lmax(lmax(T1, T3), TT);
+            st->g_tiles = lmax(lmax(lmax(T1, T3), TT), TG);
         }
     }
     __syncthreads();
     if (!s_fit) {
         if (tid == 0) {
-            st->jobs = 0; st->rows = 0; st->tiles_l3 = 0; st->tiles_b1 = 0; st->tiles_tc = 0; st->n_proj = 0;
+            st->jobs = 0; st->rows = 0; st->tiles_l3 = 0; st->tiles_b1 = 0; st->tiles_tc = 0; st->tiles_gr = 0; st->n_proj = 0;
             st->out_total = 0;
             st->ph_e[kPhPack] = globaltimer();
         }
@@ -700,12 +732,22 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
             p.tiles_tc[t] = TileDesc{j, 0, jd.n_rows, 0, jd.n_cols, (int32_t)w0, (int32_t)lmin(W, w0 + wsltc),
                                      p.djobs[j].r0};
         }
+    if (TG <= p.cap_tiles)
+        for (int64_t t = tid; t < TG; t += kPackThreads) {
+            const int64_t slice = t / totgr, local = t % totgr;
+            const int j = find_job_by_tile<4>(p.djobs, nj, local);
+            const JobDesc jd = p.jobs[j];
+            const int64_t w0 = slice * wslgr;
+            p.tiles_gr[t] = TileDesc{j, 0, jd.n_rows, 0, jd.n_cols, (int32_t)w0, (int32_t)lmin(W, w0 + wslgr),
+                                     p.djobs[j].r0};
+        }
     if (tid == 0) {
         st->jobs = nj;
         st->rows = rows_total;
         st->tiles_l3 = (int32_t)T3;
         st->tiles_b1 = (int32_t)T1;
         st->tiles_tc = (int32_t)TT;
+        st->tiles_gr = (int32_t)TG;
         st->out_total = s_out_total;
         st->max_cols = s_max_cols;
         st->max_head = s_max_head;
@@ -1362,6 +1404,7 @@ __global__ void __launch_bounds__(256) k_res_zero(const ResArgs* __restrict__ ar
         st->next3 = 0;
         st->next1 = 0;
         st->next_tc = 0;
+        st->next_gr = 0;
     }
     const int64_t n = st->out_total;
     const int64_t n4 = n >> 2;
@@ -1450,11 +1493,12 @@ struct WaveGraph {
 int build_wave_graph(WaveGraph& G, const ResArgs* d_args, ResStatus* d_status, bool with_proj, const int64_t* red_off,
                      const int32_t* red_items, cudaStream_t s) {
     G.release();
-    int sm = 148, dev = 0, occ3 = 1, occ1 = 1, occp = 1, occe = 1;
+    int sm = 148, dev = 0, occ3 = 1, occ1 = 1, occp = 1, occe = 1, occg = 1;
     TFIM_CUDA(cudaGetDevice(&dev));
     TFIM_CUDA(cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, dev));
     TFIM_TRY(persistent_occupancy(&occ3, &occ1, &occp));
     TFIM_TRY(configure_fam_kernel());
+    TFIM_TRY(occupancy_gram(&occg));
     TFIM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occe, k_res_expand_g, 256, 0));
     TFIM_CUDA(cudaGraphCreate(&G.graph, 0));
     cudaGraphConditionalHandle h;
@@ -1479,6 +1523,9 @@ int build_wave_graph(WaveGraph& G, const ResArgs* d_args, ResStatus* d_status, b
             (rc = launch_count_proj_persistent(&d_args->ap, &d_status->n_proj, sm * std::max(1, occp), red_off, red_items, s)))
             break;
         if ((rc = launch_count_fam_persistent(&d_args->atc, &d_status->tiles_tc, &d_status->next_tc, sm, s))) break;
+        if ((rc = launch_count_gram_persistent(&d_args->agr, &d_status->tiles_gr, &d_status->next_gr, sm * std::max(1, occg),
+                                               s)))
+            break;
         k_res_expand_g<<<sm * std::max(1, occe), 256, 0, s>>>(d_args);
         k_build_masks_g<<<sm * 8, 256, 0, s>>>(d_args);
         k_index_mfis_g<<<sm, 256, 0, s>>>(d_args);
@@ -1501,7 +1548,7 @@ int build_wave_graph(WaveGraph& G, const ResArgs* d_args, ResStatus* d_status, b
 
 struct ResidentState {
     Pool fams, items, heads, stack, looks, free_slots, defer, mfi_off, mfi_len, mfi_sup, mfi_items, log_feat, log_label;
-    Pool djobs, jobs, rows, row_job, row_local, tiles_l3, tiles_b1, tiles_tc, counts, status, is_root, dense_freq, top_pos,
+    Pool djobs, jobs, rows, row_job, row_local, tiles_l3, tiles_b1, tiles_tc, tiles_gr, counts, status, is_root, dense_freq, top_pos,
         top_diag, proj_list, args, top_sum, mjobs, sup_index;
     HostBuf h_status, h_args, h_res, h_setup;
     WaveGraph graph;
@@ -1509,7 +1556,7 @@ struct ResidentState {
     void release(cudaStream_t s) {
         graph.release();
         for (Pool* b : {&fams, &items, &heads, &stack, &looks, &free_slots, &defer, &mfi_off, &mfi_len, &mfi_sup, &mfi_items,
-                        &log_feat, &log_label, &djobs, &jobs, &rows, &row_job, &row_local, &tiles_l3, &tiles_b1, &tiles_tc, &counts,
+                        &log_feat, &log_label, &djobs, &jobs, &rows, &row_job, &row_local, &tiles_l3, &tiles_b1, &tiles_tc, &tiles_gr, &counts,
                         &status, &is_root, &dense_freq, &top_pos, &top_diag, &proj_list, &args, &top_sum, &mjobs,
                         &sup_index}) {
             dev_free(b->p, s);
@@ -1667,6 +1714,7 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
     TFIM_TRY(grow(R.tiles_l3, cap_tiles * sizeof(TileDesc), s));
     TFIM_TRY(grow(R.tiles_b1, cap_tiles * sizeof(TileDesc), s));
     TFIM_TRY(grow(R.tiles_tc, cap_tiles * sizeof(TileDesc), s));
+    TFIM_TRY(grow(R.tiles_gr, cap_tiles * sizeof(TileDesc), s));
     TFIM_TRY(grow(R.counts, cap_out * 4, s));
     TFIM_TRY(grow(R.is_root, is_root.size(), s));
     TFIM_TRY(grow(R.dense_freq, (size_t)std::max<int32_t>(c->info.n_dense, 1) * 4, s));
@@ -1783,6 +1831,7 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
         P.mjobs = (MaskJob*)R.mjobs.p;
         P.row_job = (int32_t*)R.row_job.p; P.row_local = (int32_t*)R.row_local.p;
         P.tiles_l3 = (TileDesc*)R.tiles_l3.p; P.tiles_b1 = (TileDesc*)R.tiles_b1.p; P.tiles_tc = (TileDesc*)R.tiles_tc.p;
+        P.tiles_gr = (TileDesc*)R.tiles_gr.p;
         P.counts = (int32_t*)R.counts.p;
         P.bitmap = c->d_bitmap; P.masks = c->d_masks.as<uint32_t>(); P.dense_freq = (const int32_t*)R.dense_freq.p;
         P.is_root = (const uint8_t*)R.is_root.p; P.st = (ResStatus*)R.status.p;
@@ -1885,6 +1934,7 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
                 TFIM_TRY(grow(R.tiles_l3, cap_tiles * sizeof(TileDesc), s));
                 TFIM_TRY(grow(R.tiles_b1, cap_tiles * sizeof(TileDesc), s));
                 TFIM_TRY(grow(R.tiles_tc, cap_tiles * sizeof(TileDesc), s));
+    TFIM_TRY(grow(R.tiles_gr, cap_tiles * sizeof(TileDesc), s));
             }
             TFIM_TRY(ensure(h, h.g_rows, h.g_jobs, h.g_out, h.g_max_head, h.g_max_cols));
         }
@@ -1927,6 +1977,7 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
             TFIM_TRY(grow(R.tiles_l3, cap_tiles * sizeof(TileDesc), s));
             TFIM_TRY(grow(R.tiles_b1, cap_tiles * sizeof(TileDesc), s));
             TFIM_TRY(grow(R.tiles_tc, cap_tiles * sizeof(TileDesc), s));
+    TFIM_TRY(grow(R.tiles_gr, cap_tiles * sizeof(TileDesc), s));
             refresh_ptrs();
         }
         if (!tl.empty())
@@ -2005,6 +2056,9 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
             a.tiles = P.tiles_tc;
             a.ph_s = &d_st->ph_s[kPhTc]; a.ph_e = &d_st->ph_e[kPhTc];
             ha->atc = a;
+            a.tiles = P.tiles_gr;
+            a.ph_s = &d_st->ph_s[kPhGram]; a.ph_e = &d_st->ph_e[kPhGram];
+            ha->agr = a;
             TFIM_CUDA(cudaMemcpyAsync(d_args, ha, sizeof(ResArgs), cudaMemcpyHostToDevice, s));
             TFIM_CUDA(cudaGraphLaunch(R.graph.exec, s));
             launches++;
@@ -2021,9 +2075,10 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
             if (hst->jobs == 0) break;   // the stack and the lookahead queue are empty
             TFIM_CHECK(slices < (1LL << 40), TFIM_E_STATE, "resident search did not finish");
         }
-        // per wave: pack, zero, lop3, b1, [proj], tc, expand, masks, index, prune, control
-        launches += (int64_t)hst->waves * (10 + (with_proj ? 1 : 0));
-        count_launches += (int64_t)hst->waves * (3 + (with_proj ? 1 : 0));
+        // per wave: pack, zero, lop3, b1, [proj], tc, gram, expand, masks, index, prune, control
+        launches += (int64_t)hst->waves * (11 + (with_proj ? 1 : 0));
+        count_launches += (int64_t)hst->waves * (4 + (with_proj ? 1 : 0));
+        path_launches[TFIM_PATH_GRAM] += hst->waves;
         path_launches[TFIM_PATH_LOP3] += hst->waves;
         path_launches[TFIM_PATH_B1] += hst->waves;
         path_launches[TFIM_PATH_TC] += hst->waves;
@@ -2075,6 +2130,15 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
             count_launches++;
             path_launches[TFIM_PATH_TC]++;
             used_tc = true;
+        }
+        if (hst->tiles_gr) {
+            a.tiles = P.tiles_gr;
+            a.n_tiles = hst->tiles_gr;
+            a.ph_s = &d_st->ph_s[kPhGram]; a.ph_e = &d_st->ph_e[kPhGram];
+            TFIM_TRY(launch_count_gram(a, s));
+            launches++;
+            count_launches++;
+            path_launches[TFIM_PATH_GRAM]++;
         }
         if (hst->n_proj) {
             a.ph_s = &d_st->ph_s[kPhProj]; a.ph_e = &d_st->ph_e[kPhProj];
@@ -2161,9 +2225,9 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
         stt->path_bitops[top_path] += top_mode == 2 ? 0 : (int64_t)n0 * (n0 + 1) / 2 * c->n_bits;
         stt->path_supports[top_path] += top_out;
         const double ns = 1e-6;
-        const int ph_of_path[5] = {kPhLop3, kPhB1, kPhTc, -1, kPhProj};
-        const int cls_of_path[5] = {kClsLop3, kClsB1, kClsTc, -1, kClsProj};
-        for (int q = 0; q < 5; q++) {
+        const int ph_of_path[6] = {kPhLop3, kPhB1, kPhTc, -1, kPhProj, kPhGram};
+        const int cls_of_path[6] = {kClsLop3, kClsB1, kClsTc, -1, kClsProj, kClsGram};
+        for (int q = 0; q < 6; q++) {
             if (ph_of_path[q] >= 0) {
                 const double ms = (double)fin.ph_ns[ph_of_path[q]] * ns;
                 stt->path_ms[q] += ms;

@@ -231,9 +231,9 @@ int main(int argc, char** argv) {
     // expansion of counted rows into children and MFIs
     printf("BMMA phase ms: mask=%g bmma=%g memcpy=%g scatter=%g\n", st.mask_ms, st.kernel_ms, st.readback_ms,
            st.expand_ms);
-    printf("count path ms: lop3=%g b1=%g tc=%g pairs=%g proj=%g  pack=%g setup=%g\n", st.path_ms[TFIM_PATH_LOP3],
-           st.path_ms[TFIM_PATH_B1], st.path_ms[TFIM_PATH_TC], st.path_ms[TFIM_PATH_PAIRS], st.path_ms[TFIM_PATH_PROJ],
-           st.pack_ms, st.setup_ms);
+    printf("count path ms: lop3=%g gram=%g b1=%g tc=%g pairs=%g proj=%g  pack=%g setup=%g\n", st.path_ms[TFIM_PATH_LOP3],
+           st.path_ms[TFIM_PATH_GRAM], st.path_ms[TFIM_PATH_B1], st.path_ms[TFIM_PATH_TC], st.path_ms[TFIM_PATH_PAIRS],
+           st.path_ms[TFIM_PATH_PROJ], st.pack_ms, st.setup_ms);
     printf("======================================================================\n");
     tfim_close(ctx);
     if (proposal) tfim_mlp_free(proposal);

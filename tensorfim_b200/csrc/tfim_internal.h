@@ -186,6 +186,15 @@ int launch_count_fam_persistent(const CountArgs* d_args, const int32_t* d_n_tile
                                 cudaStream_t s);
 int count_fam_status(bool reset);
 int configure_fam_kernel();   // opt into its shared memory (once per device, before any capture)
+// CUDA-core Gram counter for dense family jobs (count_gram.cu): a tile is one family job of at
+// most kGramMaxCols columns and at most 128 blocks of 4 x 4 (row, column) pairs, over a word
+// slice; TileDesc.pad = the F position of the job's first row.
+constexpr int kGramMaxCols = 64;
+int launch_count_gram(const CountArgs& a, cudaStream_t s);
+int launch_count_gram_persistent(const CountArgs* d_args, const int32_t* d_n_tiles, int32_t* d_next, int32_t grid,
+                                 cudaStream_t s);
+int occupancy_gram(int* blocks);
+int configure_gram_kernel();
 // The tuning table in force (common.cu): built-in values, or the table loaded / set.
 tfim_tuning tuning();
 int launch_pair_count(const int64_t* red_off, const int32_t* red_items, int64_t n_red, const int32_t* pos,

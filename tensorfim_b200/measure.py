@@ -21,9 +21,9 @@ import threading
 import time
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-PATHS = ["lop3", "b1", "tc", "pairs", "proj"]
-KERNELS = {"lop3": "k_count_lop3", "b1": "k_count_b1", "tc": "k_count_tc", "pairs": "k_pair_count",
-           "proj": "k_count_proj"}
+PATHS = ["lop3", "b1", "tc", "pairs", "proj", "gram"]
+KERNELS = {"lop3": "k_count_lop3", "b1": "k_count_b1", "tc": "k_count_fam", "pairs": "k_pair_count",
+           "proj": "k_count_proj", "gram": "k_count_gram"}
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}
 
 
@@ -61,7 +61,7 @@ def path_rooflines(stats: list[dict], hbm_gbs: float, i8_macs: float | None, sm_
              "bytes_alg_per_launch": by / launches, "bitops_per_launch": bo / launches,
              "achieved_gbs": gbs, "hbm_frac": gbs / hbm_gbs, "bitops_per_s": bo / sec if bo else 0.0,
              "share_of_counting": None}
-        if name == "lop3":
+        if name in ("lop3", "gram"):
             e["popc_frac"] = (bo / sec) / popc_ceiling(sm_count, sm_mhz)
         if name in ("b1", "tc") and i8_macs:
             e["tensor_frac"] = (bo / sec) / i8_macs

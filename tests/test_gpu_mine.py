@@ -212,3 +212,22 @@ def test_pools_handed_to_the_next_database(tmp_path):
         if k == 5:
             tf.release_cached()
     tf.release_cached(0)
+
+
+@pytest.mark.parametrize("graphs", [False, True])
+def test_dense_families_take_the_gram_and_tensor_paths(tmp_path, graphs):
+    """The dense fixture (the replicated configuration's generator at 6%) under the automatic
+    choice counts its narrow dense families with the register-tiled Gram counter and its wide
+    ones with the tcgen05 family counter; forcing the CUDA-core tiles uses neither.  Every
+    variant gives the reference's MFIs."""
+    from tensorfim_b200 import _lib
+    gram, tc = _lib.PATHS.index("gram"), _lib.PATHS.index("tc")
+    fx = load_golden("cfg3_base_t06")
+    path = golden_input(fx, tmp_path)
+    with tf.Database.from_file(path, fx["spec"]["minsup"]) as db:
+        a = db.mine(engine="resident", counter="auto", graphs=graphs)
+        assert a.as_dict() == fx["expected"]
+        assert a.stats["path_supports"][gram] > 0 and a.stats["path_supports"][tc] > 0
+        b = db.mine(engine="resident", counter="lop3", graphs=graphs)
+        assert b.as_dict() == fx["expected"]
+        assert b.stats["path_supports"][gram] == 0 and b.stats["path_supports"][tc] == 0
