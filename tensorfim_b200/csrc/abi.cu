@@ -2,6 +2,7 @@
 #include <unistd.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -32,8 +33,11 @@ int make_ctx(int32_t device, tfim_ctx** out) {
     tfim_ctx* c = new (std::nothrow) tfim_ctx();
     TFIM_CHECK(c != nullptr, TFIM_E_NOMEM, "context allocation failed");
     c->device = device;
+    static std::atomic<uint64_t> next_uid{1};
+    c->uid = next_uid.fetch_add(1);
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
+        cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
+        cudaEventCreate(&c->ev_span0) != cudaSuccess || cudaEventCreate(&c->ev_span1) != cudaSuccess) {
         set_error("stream/event creation failed: %s", cudaGetErrorString(cudaGetLastError()));
         tfim_close(c);
         return TFIM_E_CUDA;
@@ -357,9 +361,7 @@ int tfim_mine(tfim_ctx* c, const tfim_mine_opts* opts, tfim_mine_stats* stats) {
     memset(&st, 0, sizeof st);
     c->mfis.clear();
     c->mined = false;
-    cudaEvent_t e_begin = nullptr, e_end = nullptr;
-    TFIM_CUDA(cudaEventCreate(&e_begin));
-    TFIM_CUDA(cudaEventCreate(&e_end));
+    cudaEvent_t e_begin = c->ev_span0, e_end = c->ev_span1;
     TFIM_CUDA(cudaEventRecord(e_begin, c->stream));
     const auto t0 = std::chrono::steady_clock::now();
     int rc;
@@ -371,8 +373,6 @@ int tfim_mine(tfim_ctx* c, const tfim_mine_opts* opts, tfim_mine_stats* stats) {
     const auto t1 = std::chrono::steady_clock::now();
     float span_ms = 0;
     cudaEventElapsedTime(&span_ms, e_begin, e_end);
-    cudaEventDestroy(e_begin);
-    cudaEventDestroy(e_end);
     if (rc != TFIM_OK) return rc;
     st.device_ms = span_ms;
     st.host_ms = std::chrono::duration<double, std::milli>(t1 - t0).count() - st.sync_ms;
@@ -535,6 +535,8 @@ void tfim_close(tfim_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->ev_span0) cudaEventDestroy(c->ev_span0);
+    if (c->ev_span1) cudaEventDestroy(c->ev_span1);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }

@@ -1551,6 +1551,13 @@ struct ResidentState {
     Pool djobs, jobs, rows, row_job, row_local, tiles_l3, tiles_b1, tiles_tc, tiles_gr, counts, status, is_root, dense_freq, top_pos,
         top_diag, proj_list, args, top_sum, mjobs, sup_index;
     HostBuf h_status, h_args, h_res, h_setup;
+    // the database's part of the search's initial state (root flags, the top family in
+    // increasing support order), computed at a context's first resident mine and its pinned
+    // staging reused by later mines; setup_uid names the context it belongs to
+    uint64_t setup_uid = 0;
+    std::vector<char> is_root_h;
+    std::vector<int32_t> F0;
+    size_t setup_total = 0;
     WaveGraph graph;
     int32_t launch_id = 0;
     void release(cudaStream_t s) {
@@ -1654,16 +1661,21 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
     c->la_feats.clear();
     c->la_labels.clear();
 
+    const bool fresh_setup = R.setup_uid != c->uid;
+    if (fresh_setup) {
+        R.is_root_h.assign((size_t)c->info.n_dense + 1, 0);
+        for (int32_t r : c->roots) R.is_root_h[r] = 1;
+        // top family: the counted items frequent by bitmap support, increasing support
+        R.F0.clear();
+        for (int32_t e = 0; e < d; e++)
+            if (c->bit_support[e] >= minc) R.F0.push_back(e);
+        std::stable_sort(R.F0.begin(), R.F0.end(),
+                         [&](int32_t a, int32_t b) { return c->bit_support[a] < c->bit_support[b]; });
+    }
+    const std::vector<char>& is_root = R.is_root_h;
+    const std::vector<int32_t>& F0 = R.F0;
     // the parked id 0 used as a root: the reference's search for that root (host driver)
-    std::vector<char> is_root((size_t)c->info.n_dense + 1, 0);
-    for (int32_t r : c->roots) is_root[r] = 1;
     if (c->info.n_dense > d && is_root[d]) TFIM_TRY(mine_plain_roots(c, {d}, stt));
-
-    // top family: the counted items frequent by bitmap support, increasing support
-    std::vector<int32_t> F0;
-    for (int32_t e = 0; e < d; e++)
-        if (c->bit_support[e] >= minc) F0.push_back(e);
-    std::stable_sort(F0.begin(), F0.end(), [&](int32_t a, int32_t b) { return c->bit_support[a] < c->bit_support[b]; });
     const int32_t n0 = (int32_t)F0.size();
     if (n0 == 0) return TFIM_OK;
 
@@ -1750,6 +1762,8 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
     hs.nodes = n0;
     hs.supports = (unsigned long long)top_out;
     {
+        // the staging blob is the same for every mine of this database: built once, and the
+        // parts (whose device pools may have moved) copied again on every mine
         const size_t nd = (size_t)std::max<int32_t>(c->info.n_dense, 1);
         struct Part { void* dst; size_t off, bytes; };
         std::vector<Part> parts;
@@ -1765,29 +1779,35 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
                      p_rows = part(R.rows.p, (size_t)n0 * sizeof(RowDesc)), p_rj = part(R.row_job.p, (size_t)n0 * 4),
                      p_rl = part(R.row_local.p, (size_t)n0 * 4), p_pos = part(R.top_pos.p, nd * 4),
                      p_diag = part(R.top_diag.p, (size_t)n0 * 4), p_st = part(R.status.p, sizeof(ResStatus));
-        TFIM_TRY(R.h_setup.reserve(total));
-        unsigned char* h = R.h_setup.as<unsigned char>();
-        auto at = [&](size_t k) { return (void*)(h + parts[k].off); };
-        memcpy(at(p_root), is_root.data(), is_root.size());
-        memcpy(at(p_freq), c->dense_freq.data(), c->dense_freq.size() * 4);
-        memcpy(at(p_fam), &top, sizeof top);
-        memcpy(at(p_F), F0.data(), (size_t)n0 * 4);
-        *(DJob*)at(p_dj) = DJob{0, kJobFam, 0, n0, -1, -1, 0, 0, 0, 1, 0, 0};
-        *(JobDesc*)at(p_jd) = JobDesc{-1, -1, n0, n0, 0, 0, 0, -1, 0};
-        RowDesc* rows = (RowDesc*)at(p_rows);
-        int32_t* rj = (int32_t*)at(p_rj);
-        int32_t* rl = (int32_t*)at(p_rl);
-        int32_t* pos = (int32_t*)at(p_pos);
-        int32_t* diag = (int32_t*)at(p_diag);
-        std::fill(pos, pos + nd, -1);
-        for (int32_t k = 0; k < n0; k++) {
-            rows[k] = RowDesc{-1, F0[k]};
-            rj[k] = 0;
-            rl[k] = k;
-            pos[F0[k]] = k;
-            diag[k] = c->bit_support[F0[k]];
+        unsigned char* h = nullptr;
+        if (fresh_setup || !R.h_setup.p || R.setup_total != total) {
+            TFIM_TRY(R.h_setup.reserve(total));
+            h = R.h_setup.as<unsigned char>();
+            auto at = [&](size_t k) { return (void*)(h + parts[k].off); };
+            memcpy(at(p_root), is_root.data(), is_root.size());
+            memcpy(at(p_freq), c->dense_freq.data(), c->dense_freq.size() * 4);
+            memcpy(at(p_fam), &top, sizeof top);
+            memcpy(at(p_F), F0.data(), (size_t)n0 * 4);
+            *(DJob*)at(p_dj) = DJob{0, kJobFam, 0, n0, -1, -1, 0, 0, 0, 1, 0, 0, 0, 0};
+            *(JobDesc*)at(p_jd) = JobDesc{-1, -1, n0, n0, 0, 0, 0, -1, 0};
+            RowDesc* rows = (RowDesc*)at(p_rows);
+            int32_t* rj = (int32_t*)at(p_rj);
+            int32_t* rl = (int32_t*)at(p_rl);
+            int32_t* pos = (int32_t*)at(p_pos);
+            int32_t* diag = (int32_t*)at(p_diag);
+            std::fill(pos, pos + nd, -1);
+            for (int32_t k = 0; k < n0; k++) {
+                rows[k] = RowDesc{-1, F0[k]};
+                rj[k] = 0;
+                rl[k] = k;
+                pos[F0[k]] = k;
+                diag[k] = c->bit_support[F0[k]];
+            }
+            memcpy(at(p_st), &hs, sizeof hs);
+            R.setup_uid = c->uid;
+            R.setup_total = total;
         }
-        memcpy(at(p_st), &hs, sizeof hs);
+        h = R.h_setup.as<unsigned char>();
         for (const Part& q : parts)
             if (q.bytes) TFIM_CUDA(cudaMemcpyAsync(q.dst, h + q.off, q.bytes, cudaMemcpyHostToDevice, s));
     }

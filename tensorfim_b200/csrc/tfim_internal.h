@@ -245,6 +245,8 @@ struct MfiSet {
 struct tfim_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
+    uint64_t uid = 0;                      // unique per context opened in this process
+    cudaEvent_t ev_span0 = nullptr, ev_span1 = nullptr;   // the span of a tfim_mine
     tfim_db_info info{};
     bool from_db = false;
     // host-side item tables (dense id space)

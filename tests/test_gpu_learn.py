@@ -88,8 +88,8 @@ def test_lookahead_log_records_outcomes(tmp_path, engine):
 @pytest.mark.skipif(not os.path.exists(learn.WEIGHTS), reason="trained weights not present")
 def test_learned_proposal_gain_on_cfg5():
     """Evaluation database of the learned proposal (2,000,000 tx x 60 groups, minsup 70%):
-    the trained network issues fewer lookaheads that miss than the filtered policy, keeps
-    the output identical to the plain engine."""
+    the trained network keeps the output identical to the plain engine and issues no more
+    lookaheads that miss than the filtered policy."""
     db0 = synth.generate(5)
     with tf.Database.from_csr(db0.offsets, db0.items, 0.70) as db:
         plain = db.mine(engine="plain").as_dict()
@@ -99,4 +99,24 @@ def test_learned_proposal_gain_on_cfg5():
         wasted_base = base.stats["lookaheads"] - base.stats["lookahead_hits"]
         wasted_lrn = lrn.stats["lookaheads"] - lrn.stats["lookahead_hits"]
         assert wasted_lrn <= wasted_base
-        assert lrn.stats["supports"] <= base.stats["supports"] * 1.10
+        assert lrn.stats["supports"] <= base.stats["supports"]
+
+
+@pytest.mark.slow
+@pytest.mark.skipif(not os.path.exists(learn.WEIGHTS), reason="trained weights not present")
+@pytest.mark.parametrize("cfg,kw,minsup", [(3, dict(replicas=1), 0.06), (4, dict(scale=0.25), 0.0005)])
+def test_learned_proposal_strictly_beats_the_filter(cfg, kw, minsup):
+    """Where lookaheads matter -- the replicated configuration's generator at 6% (40,760
+    nodes) and the sparse configuration at a quarter of its rows -- the trained network
+    issues strictly fewer lookaheads that miss than the tail-pair filter and the search
+    counts strictly fewer supports, with the same MFIs as the plain engine."""
+    db0 = synth.generate(cfg, **kw)
+    with tf.Database.from_csr(db0.offsets, db0.items, minsup) as db:
+        plain = db.mine(engine="plain").as_dict()
+        base = db.mine(lookahead="filtered")
+        lrn = db.mine(lookahead="learned")
+        assert lrn.as_dict() == plain and base.as_dict() == plain
+        wasted_base = base.stats["lookaheads"] - base.stats["lookahead_hits"]
+        wasted_lrn = lrn.stats["lookaheads"] - lrn.stats["lookahead_hits"]
+        assert wasted_lrn < wasted_base, (wasted_lrn, wasted_base)
+        assert lrn.stats["supports"] < base.stats["supports"], (lrn.stats["supports"], base.stats["supports"])
