@@ -5,14 +5,17 @@
 // the job is a small Gram block of X_c = base & B[F[c]] (at most kGramMaxCols columns).  The
 // arithmetic is the reference's per-node count (code/engine/src/kernel_bitmap.cu:390-442:
 // popc of ANDed bit rows summed over the transaction words); the schedule is a GEMM's:
-//   * a tile is one job over a word slice; a CTA of 128 threads stages X for a chunk of 32
-//     128-bit positions in shared memory (rows padded by 16 bytes), double-buffered, while
-//     the next chunk's words are loaded into registers;
-//   * each thread owns a 4 x 4 block of (row, column) pairs and a subset of the chunk's
-//     positions: per position 8 shared loads of 16 bytes feed 64 popc, so the POPC pipe (16
-//     per SM and clock) bounds it rather than loads or staging;
-//   * at the end of the tile the threads of a block reduce their sums with shuffles and one
-//     lane adds each pair's count to the job's output (word slices of one job meet there).
+//   * a tile is one job over a word slice; a CTA of 128 threads stages X for a chunk of 32 to
+//     256 128-bit positions (fewer columns, more positions) in shared memory, rows padded by
+//     16 bytes, double-buffered, while the next chunk's words are loaded into registers;
+//   * each thread owns a block of 16 (row, column) pairs -- 4 x 4, or 2 x 8 / 1 x 16 for tails
+//     of 2 / 1 rows -- and a subset of the chunk's positions: per position 8 to 17 shared loads
+//     of 16 bytes feed 64 popc, so the POPC pipe (16 per SM and clock) bounds it rather than
+//     loads or staging;
+//   * at the end of the tile the threads of a block add their sums in shared memory and one
+//     thread adds each pair's count to the job's output (word slices of one job meet there).
+// Measured on one B200 (one job, 4.2 Mbit rows, CUDA events): 86-91% of the POPC ceiling at
+// 32 and 64 columns.
 #include <atomic>
 
 #include "tfim_internal.h"
@@ -21,110 +24,146 @@ namespace tfim {
 namespace {
 
 constexpr int kGThreads = 128;
-constexpr int kGPos = 32;                              // 128-bit positions per chunk
-constexpr int kGRowStride = kGPos * 16 + 16;           // bytes per staged row (padded)
-// one chunk of every column, plus 4 rows: a 4 x 4 pair block at the edge reads rows up to
-// nF + 2 (its results are discarded), which stays inside the buffer
-constexpr int kGBuf = (kGramMaxCols + 4) * kGRowStride;
-constexpr int kGSmem = 2 * kGBuf;
-constexpr int kGUnits = kGramMaxCols * kGPos / kGThreads;   // staged words per thread and chunk (16)
+constexpr int kGUnits = 16;                            // staged words per thread and chunk
+// positions (128-bit words) per chunk by the family's width: kGUnits * kGThreads words of
+// staging, every column of the chunk
+__host__ __device__ __forceinline__ int gram_positions(int nF) {
+    return nF <= 8 ? 256 : nF <= 16 ? 128 : nF <= 32 ? 64 : 32;
+}
+// one chunk of every column (a pair block at the edge reads its rows and columns clamped to
+// the last column, and its results there are discarded)
+constexpr int kGBuf = 64 * (32 * 16 + 16);
+static_assert(8 * (256 * 16 + 16) <= kGBuf && 16 * (128 * 16 + 16) <= kGBuf && 32 * (64 * 16 + 16) <= kGBuf,
+              "every chunk shape fits a buffer");
+constexpr int kGSmem = 2 * kGBuf + kGThreads * 16 * 4;   // two buffers + the final sums
 
 __device__ __forceinline__ uint32_t popc4and(uint4 a, uint4 b) {
     return __popc(a.x & b.x) + __popc(a.y & b.y) + __popc(a.z & b.z) + __popc(a.w & b.w);
 }
 
-__device__ void gram_tile(const CountArgs& a, const TileDesc t, uint8_t* smem) {
+// Pair blocks of BR rows x BC columns (BR * BC = 16): a tail of 1 or 2 rows takes 1 x 16 or
+// 2 x 8 blocks, longer tails 4 x 4, so few pairs of a block fall outside the job.
+template <int BR>
+__device__ void gram_tile_t(const CountArgs& a, const TileDesc t, uint8_t* smem) {
+    constexpr int BC = 16 / BR;
     const JobDesc j = a.jobs[t.job];
     const int64_t W = a.W;
     const int tid = threadIdx.x;
     const int nF = t.c1, nr = t.nr, s0 = t.pad;
+    const int P = gram_positions(nF);
+    const int stride = P * 16 + 16;
     const uint32_t* bm = j.base_slot >= 0 ? a.masks + (int64_t)j.base_slot * W : nullptr;
     const uint32_t* bi = j.base_item >= 0 ? a.bitmap + (int64_t)j.base_item * W : nullptr;
-    // this thread's staged units: position p (fixed), columns c = tid / 32 + 4 * u
-    const int p_ld = tid & (kGPos - 1), c_ld0 = tid >> 5;
-    const int n_ld = (nF - c_ld0 + 3) >> 2;   // <= kGUnits
+    // staged unit u = tid + kGThreads * k: column u / P, position u % P (at most 2 positions
+    // per thread, at 256 positions)
     const uint32_t* src[kGUnits];
+    int ucol[kGUnits], upos[kGUnits];
 #pragma unroll
-    for (int u = 0; u < kGUnits; u++)
-        src[u] = u < n_ld ? a.bitmap + (int64_t)a.cols[j.col_off + c_ld0 + 4 * u] * W : nullptr;
-    // pair blocks of 4 rows x 4 columns; G threads per block share its positions
-    const int rb = (nr + 3) >> 2, cb = (nF + 3) >> 2, nb = rb * cb;   // nb <= kGThreads
-    int G = 1;
-    while (G * 2 * nb <= kGThreads && G < kGPos) G *= 2;
-    const int b = tid / G, g = tid % G;
+    for (int k = 0; k < kGUnits; k++) {
+        const int u = tid + kGThreads * k;
+        ucol[k] = u / P;
+        upos[k] = u % P;
+        src[k] = ucol[k] < nF ? a.bitmap + (int64_t)a.cols[j.col_off + ucol[k]] * W : nullptr;
+    }
+    // pair blocks; G threads per block share its positions (G need not be a power of two)
+    const int rb = (nr + BR - 1) / BR, cb = (nF + BC - 1) / BC, nb = rb * cb;   // nb <= kGThreads
+    const int G = min(P, kGThreads / nb);
+    const int b = tid / G, g = tid - b * G;
     const bool busy = b < nb;
-    const int br = busy ? (b / cb) * 4 : 0, bc = busy ? (b % cb) * 4 : 0;
-    uint32_t acc[4][4];
+    const int br = busy ? (b / cb) * BR : 0, bc = busy ? (b % cb) * BC : 0;
+    uint32_t acc[BR][BC];
 #pragma unroll
-    for (int x = 0; x < 4; x++)
+    for (int x = 0; x < BR; x++)
 #pragma unroll
-        for (int y = 0; y < 4; y++) acc[x][y] = 0;
+        for (int y = 0; y < BC; y++) acc[x][y] = 0;
+    // byte offsets of the block's rows and columns within a staged chunk, clamped to the
+    // last column (pairs outside the job are computed on valid rows and discarded)
+    int rofs[BR], cofs[BC];
+#pragma unroll
+    for (int x = 0; x < BR; x++) rofs[x] = min(s0 + br + x, nF - 1) * stride;
+#pragma unroll
+    for (int y = 0; y < BC; y++) cofs[y] = min(bc + y, nF - 1) * stride;
+    int32_t* sums = reinterpret_cast<int32_t*>(smem + 2 * kGBuf);   // (row, column) -> sum
+    for (int q = tid; q < kGThreads * 16; q += kGThreads) sums[q] = 0;
 
     const int64_t P0 = t.w0 >> 2, P1 = t.w1 >> 2;   // 128-bit positions of the slice
-    const int n_ch = (int)((P1 - P0 + kGPos - 1) / kGPos);
+    const int n_ch = (int)((P1 - P0 + P - 1) / P);
     uint4 pre[kGUnits];
-    uint4 pbase = make_uint4(~0u, ~0u, ~0u, ~0u);
-    auto load = [&](int ch) {
-        const int64_t p = P0 + (int64_t)ch * kGPos + p_ld;
-        const bool in = ch < n_ch && p < P1;
-        pbase = make_uint4(~0u, ~0u, ~0u, ~0u);
-        if (in && bm) pbase = __ldg(reinterpret_cast<const uint4*>(bm) + p);
-        if (in && bi) {
+    uint4 pb0 = make_uint4(~0u, ~0u, ~0u, ~0u), pb1 = pb0;   // base words of this thread's positions
+    const int pa = upos[0], pbp = upos[kGUnits - 1];         // its (at most) two positions
+    auto base_at = [&](int64_t p) {
+        uint4 x = make_uint4(~0u, ~0u, ~0u, ~0u);
+        if (bm) x = __ldg(reinterpret_cast<const uint4*>(bm) + p);
+        if (bi) {
             const uint4 v = __ldg(reinterpret_cast<const uint4*>(bi) + p);
-            pbase = make_uint4(pbase.x & v.x, pbase.y & v.y, pbase.z & v.z, pbase.w & v.w);
+            x = make_uint4(x.x & v.x, x.y & v.y, x.z & v.z, x.w & v.w);
         }
+        return x;
+    };
+    auto load = [&](int ch) {
+        const int64_t c0 = P0 + (int64_t)ch * P;
+        if (ch < n_ch && c0 + pa < P1) pb0 = base_at(c0 + pa);
+        if (ch < n_ch && c0 + pbp < P1 && pbp != pa) pb1 = base_at(c0 + pbp);
 #pragma unroll
-        for (int u = 0; u < kGUnits; u++)
-            pre[u] = (in && u < n_ld) ? __ldg(reinterpret_cast<const uint4*>(src[u]) + p) : make_uint4(0, 0, 0, 0);
+        for (int k = 0; k < kGUnits; k++) {
+            const int64_t p = c0 + upos[k];
+            pre[k] = (ch < n_ch && src[k] && p < P1) ? __ldg(reinterpret_cast<const uint4*>(src[k]) + p)
+                                                     : make_uint4(0, 0, 0, 0);
+        }
     };
     load(0);
     for (int ch = 0; ch < n_ch; ch++) {
         uint8_t* buf = smem + (ch & 1) * kGBuf;
 #pragma unroll
-        for (int u = 0; u < kGUnits; u++)
-            if (u < n_ld) {
-                const uint4 v = pre[u];
-                *reinterpret_cast<uint4*>(buf + (c_ld0 + 4 * u) * kGRowStride + p_ld * 16) =
-                    make_uint4(v.x & pbase.x, v.y & pbase.y, v.z & pbase.z, v.w & pbase.w);
+        for (int k = 0; k < kGUnits; k++)
+            if (ucol[k] < nF) {
+                const uint4 v = pre[k];
+                const uint4 bw = upos[k] == pa ? pb0 : pb1;
+                *reinterpret_cast<uint4*>(buf + ucol[k] * stride + upos[k] * 16) =
+                    make_uint4(v.x & bw.x, v.y & bw.y, v.z & bw.z, v.w & bw.w);
             }
         __syncthreads();
         if (ch + 1 < n_ch) load(ch + 1);   // in flight during this chunk's popc
-        const int64_t rem_p = P1 - (P0 + (int64_t)ch * kGPos);
-        const int np = rem_p < kGPos ? (int)rem_p : kGPos;
+        const int64_t rem_p = P1 - (P0 + (int64_t)ch * P);
+        const int np = rem_p < P ? (int)rem_p : P;
         if (busy) {
             for (int p = g; p < np; p += G) {
-                uint4 xr[4], xc[4];
+                uint4 xr[BR], xc[BC];
 #pragma unroll
-                for (int x = 0; x < 4; x++) {
-                    xr[x] = *reinterpret_cast<const uint4*>(buf + (s0 + br + x) * kGRowStride + p * 16);
-                    xc[x] = *reinterpret_cast<const uint4*>(buf + (bc + x) * kGRowStride + p * 16);
-                }
+                for (int x = 0; x < BR; x++) xr[x] = *reinterpret_cast<const uint4*>(buf + rofs[x] + p * 16);
 #pragma unroll
-                for (int x = 0; x < 4; x++)
+                for (int y = 0; y < BC; y++) xc[y] = *reinterpret_cast<const uint4*>(buf + cofs[y] + p * 16);
 #pragma unroll
-                    for (int y = 0; y < 4; y++) acc[x][y] += popc4and(xr[x], xc[y]);
+                for (int x = 0; x < BR; x++)
+#pragma unroll
+                    for (int y = 0; y < BC; y++) acc[x][y] += popc4and(xr[x], xc[y]);
             }
         }
         // the next iteration writes the other buffer; the one after it, this one, only after
         // every thread passed the next iteration's barrier (and so finished this chunk)
     }
-    // sums over the G threads of a block (consecutive lanes of one warp)
+    // sums over the G threads of each block in shared memory, then one atomic per pair
+    if (busy) {
 #pragma unroll
-    for (int x = 0; x < 4; x++)
+        for (int x = 0; x < BR; x++)
 #pragma unroll
-        for (int y = 0; y < 4; y++)
-            for (int o = 1; o < G; o <<= 1) acc[x][y] += __shfl_xor_sync(0xffffffffu, acc[x][y], o);
-    if (busy && g == 0) {
-#pragma unroll
-        for (int x = 0; x < 4; x++)
-#pragma unroll
-            for (int y = 0; y < 4; y++) {
-                const int r = br + x, c = bc + y;
-                if (r < nr && c < nF && acc[x][y])
-                    atomicAdd(a.out + j.out_off + (int64_t)(t.r0 + r) * j.n_cols + c, (int32_t)acc[x][y]);
-            }
+            for (int y = 0; y < BC; y++)
+                if (acc[x][y]) atomicAdd(&sums[b * 16 + x * BC + y], (int32_t)acc[x][y]);
     }
-    __syncthreads();   // the block's next tile reuses the buffers
+    __syncthreads();
+    for (int q = tid; q < nb * 16; q += kGThreads) {
+        const int bb = q >> 4, x = (q & 15) / BC, y = (q & 15) % BC;
+        const int r = (bb / cb) * BR + x, c = (bb % cb) * BC + y;
+        const int32_t v = sums[q];
+        if (r < nr && c < nF && v) atomicAdd(a.out + j.out_off + (int64_t)(t.r0 + r) * j.n_cols + c, v);
+    }
+    __syncthreads();   // the block's next tile reuses the buffers and the sums
+}
+
+__device__ __forceinline__ void gram_tile(const CountArgs& a, const TileDesc t, uint8_t* smem) {
+    if (t.nr <= 1) gram_tile_t<1>(a, t, smem);
+    else if (t.nr <= 2) gram_tile_t<2>(a, t, smem);
+    else gram_tile_t<4>(a, t, smem);
 }
 
 __global__ void __launch_bounds__(kGThreads) k_count_gram(CountArgs a) {
