@@ -159,7 +159,7 @@ void tuning_builtin(tfim_tuning* t) {
     t->i8_min_rows = 128;
     t->i8_min_cols = 128;
     t->rate_i8_bitops = 3.0e14;
-    t->tc_min_work = 512;
+    t->tc_min_work = 1536;
     t->tc_min_density = 0.5f;
     t->tc_tiles_per_sm = 8.f;
 }

@@ -215,6 +215,9 @@ __device__ __forceinline__ bool use_tc(const ResPtrs& p, const JobDesc& jd, int3
     if (jd.n_cols < 1 || jd.n_cols > kFamMaxCols || jd.n_rows < 1) return false;
     if (p.counter == TFIM_COUNTER_I8) return true;
     if (p.counter != TFIM_COUNTER_AUTO) return false;
+    // families up to kGramMaxCols columns are the Gram counter's (measured faster at every
+    // shape there); wider ones take the tensor tiles when large enough to fill their MMAs
+    if (jd.n_cols <= kGramMaxCols) return false;
     if ((int64_t)jd.n_rows * jd.n_cols < p.tc_min_work) return false;
     const float d = p.n_bits > 0 ? fminf(1.f, 128.f * (float)sup / (float)p.n_bits) : 1.f;
     return d >= p.tc_min_density;
@@ -225,7 +228,9 @@ __device__ __forceinline__ bool use_tc(const ResPtrs& p, const JobDesc& jd, int3
 // skip, and at these widths the register-tiled Gram block (86-91% of the POPC ceiling at 32
 // and 64 columns) beats the tensor tiles, whose narrow MMAs cost about 50 cycles each.
 __device__ __forceinline__ bool use_gram(const ResPtrs& p, const JobDesc& jd, int32_t sup) {
-    if (jd.n_cols < 1 || jd.n_cols > kGramMaxCols || jd.n_rows < 1) return false;
+    // tails of 1 or 2 rows are memory-bound in any kernel (8 bit-ops per byte and row); the
+    // general tiles handle them as well, and measured faster on the dense benchmark
+    if (jd.n_cols < 1 || jd.n_cols > kGramMaxCols || jd.n_rows < 3) return false;
     if (((jd.n_rows + 3) / 4) * ((jd.n_cols + 3) / 4) > 128) return false;
     if (p.counter != TFIM_COUNTER_AUTO) return false;
     const float d = p.n_bits > 0 ? fminf(1.f, 128.f * (float)sup / (float)p.n_bits) : 1.f;
