@@ -316,7 +316,8 @@ typedef struct {
                                    at most 128 columns with rows x columns >= tc_min_work and a */
     float   tc_min_density;     /*   prefix holding at least this fraction of 128-bit positions */
     float   tc_tiles_per_sm;    /* tcgen05 family counter: word-slice tiles per SM and wave */
-    int32_t reserved[1];
+    int32_t gram_min_rows;      /* automatic choice: the CUDA-core Gram counter for dense family
+                                   jobs of at most 64 columns and at least this many rows */
 } tfim_tuning;
 
 /* The table in force (built-in values, or the loaded / set table). */

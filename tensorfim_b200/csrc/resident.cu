@@ -155,6 +155,7 @@ struct ResPtrs {
     float l3_slices_per_sm, b1_tiles_per_sm;   // work split targets per wave
     int32_t tc_min_work;                       // automatic choice of the tcgen05 family counter
     float tc_min_density, tc_tiles_per_sm;
+    int32_t gram_min_rows;                     // ... and of the CUDA-core Gram counter
     Caps caps;
     int64_t row_bytes;            // bytes of one bitmap row (algorithmic traffic accounting)
     const struct RowSum* row_sum; // first pass of the expand precomputed per wave row (or nullptr)
@@ -230,7 +231,7 @@ __device__ __forceinline__ bool use_tc(const ResPtrs& p, const JobDesc& jd, int3
 __device__ __forceinline__ bool use_gram(const ResPtrs& p, const JobDesc& jd, int32_t sup) {
     // tails of 1 or 2 rows are memory-bound in any kernel (8 bit-ops per byte and row); the
     // general tiles handle them as well, and measured faster on the dense benchmark
-    if (jd.n_cols < 1 || jd.n_cols > kGramMaxCols || jd.n_rows < 3) return false;
+    if (jd.n_cols < 1 || jd.n_cols > kGramMaxCols || jd.n_rows < p.gram_min_rows) return false;
     if (((jd.n_rows + 3) / 4) * ((jd.n_cols + 3) / 4) > 128) return false;
     if (p.counter != TFIM_COUNTER_AUTO) return false;
     const float d = p.n_bits > 0 ? fminf(1.f, 128.f * (float)sup / (float)p.n_bits) : 1.f;
@@ -1876,6 +1877,7 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
         P.tc_min_work = tn.tc_min_work;
         P.tc_min_density = tn.tc_min_density;
         P.tc_tiles_per_sm = tn.tc_tiles_per_sm;
+        P.gram_min_rows = tn.gram_min_rows;
         if (la_mode == 2 && c->proposal) {
             const void* wb = nullptr;
             const float* pp = nullptr;
