@@ -1555,7 +1555,7 @@ int build_wave_graph(WaveGraph& G, const ResArgs* d_args, ResStatus* d_status, b
 
 struct ResidentState {
     Pool fams, items, heads, stack, looks, free_slots, defer, mfi_off, mfi_len, mfi_sup, mfi_items, log_feat, log_label;
-    Pool djobs, jobs, rows, row_job, row_local, tiles_l3, tiles_b1, tiles_tc, tiles_gr, counts, status, is_root, dense_freq, top_pos,
+    Pool djobs, jobs, rows, row_job, row_local, tiles_l3, tiles_b1, tiles_tc, tiles_gr, counts, status, is_root, dense_freq, top_pos, top_tri,
         top_diag, proj_list, args, top_sum, mjobs, sup_index;
     HostBuf h_status, h_args, h_res, h_setup;
     // the database's part of the search's initial state (root flags, the top family in
@@ -1570,7 +1570,7 @@ struct ResidentState {
     void release(cudaStream_t s) {
         graph.release();
         for (Pool* b : {&fams, &items, &heads, &stack, &looks, &free_slots, &defer, &mfi_off, &mfi_len, &mfi_sup, &mfi_items,
-                        &log_feat, &log_label, &djobs, &jobs, &rows, &row_job, &row_local, &tiles_l3, &tiles_b1, &tiles_tc, &tiles_gr, &counts,
+                        &log_feat, &log_label, &djobs, &jobs, &rows, &row_job, &row_local, &tiles_l3, &tiles_b1, &tiles_tc, &tiles_gr, &counts, &top_tri,
                         &status, &is_root, &dense_freq, &top_pos, &top_diag, &proj_list, &args, &top_sum, &mjobs,
                         &sup_index}) {
             dev_free(b->p, s);
@@ -2011,14 +2011,22 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
         if (!tl.empty())
             TFIM_CUDA(cudaMemcpyAsync(top_b1 ? R.tiles_b1.p : R.tiles_l3.p, tl.data(), tl.size() * sizeof(TileDesc),
                                       cudaMemcpyHostToDevice, s));
-        TFIM_CUDA(cudaMemsetAsync(R.counts.p, 0, (size_t)top_out * 4, s));
+        const int64_t tri = pair_triangle_entries(n0);
+        if (top_mode == 2) {
+            // pairs into the packed triangle; the mirror below writes every entry of the block
+            TFIM_TRY(grow(R.top_tri, (size_t)std::max<int64_t>(tri, 4) * 4, s));
+            TFIM_CUDA(cudaMemsetAsync(R.top_tri.p, 0, (size_t)tri * 4, s));
+        } else {
+            TFIM_CUDA(cudaMemsetAsync(R.counts.p, 0, (size_t)top_out * 4, s));
+        }
         CountArgs a;
         a.bitmap = c->d_bitmap; a.W = W; a.masks = c->d_masks.as<uint32_t>(); a.jobs = P.jobs; a.rows = P.rows;
         a.cols = P.items; a.out = P.counts;
         stt->setup_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_entry).count();
         TFIM_CUDA(cudaEventRecord(c->ev0, s));
         if (top_mode == 2) {
-            TFIM_TRY(launch_pair_count(c->d_red_off, c->d_red_items, c->n_bits, (const int32_t*)R.top_pos.p, n0, P.counts, s));
+            TFIM_TRY(launch_pair_count(c->d_red_off, c->d_red_items, c->n_bits, (const int32_t*)R.top_pos.p, n0,
+                                       (int32_t*)R.top_tri.p, s));
             bytes_alg += (c->n_bits + 1) * 8 + c->n_red_items * 4 + 4 * top_out;
         } else {
             a.tiles = top_b1 ? P.tiles_b1 : P.tiles_l3;
@@ -2027,7 +2035,8 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
             bytes_alg += row_bytes * 2 * n0 + 4 * top_out;
         }
         TFIM_CUDA(cudaEventRecord(c->ev1, s));
-        TFIM_TRY(launch_mirror(P.counts, n0, top_mode == 2 ? (const int32_t*)R.top_diag.p : nullptr, s));
+        if (top_mode == 2) TFIM_TRY(launch_mirror_tri((const int32_t*)R.top_tri.p, P.counts, n0, (const int32_t*)R.top_diag.p, s));
+        else TFIM_TRY(launch_mirror(P.counts, n0, nullptr, s));
         TFIM_TRY(grow(R.top_sum, (size_t)n0 * sizeof(RowSum), s));
         k_top_summary<<<n0, 256, 0, s>>>(P.counts, n0, minc, (RowSum*)R.top_sum.p);
         TFIM_CUDA(cudaGetLastError());
