@@ -9,23 +9,60 @@
 // sum over rows of len^2/2 increments instead of d^2 x N/2 bit operations.  The engine
 // picks it per database from those two work estimates.  Counts are exact integers either
 // way.
+#include <algorithm>
+
 #include "tfim_internal.h"
 
 namespace tfim {
 namespace {
 
-// Index of pair (i, j), i < j, in the packed upper triangle of an nF x nF matrix.
-__device__ __forceinline__ int64_t tri_index(int32_t i, int32_t j, int32_t nF) {
-    return (int64_t)i * (2 * (int64_t)nF - i - 1) / 2 + (j - i - 1);
+// Offset of row i of the packed triangle, less i + 1: pair (i, j) sits at tri_row(i) + j.
+__device__ __forceinline__ int64_t tri_row(int32_t i, int32_t nF) {
+    return (int64_t)i * (2 * (int64_t)nF - i - 1) / 2 - i - 1;
 }
+
+constexpr int kPairThreads = 256;
+constexpr int kPairRow = 32;   // frequent items of a reduced row held in shared memory
 
 // One thread per reduced row: every pair (a, b) of items of the row that are in F adds 1
 // to the packed upper triangle T at (min(pos), max(pos)).  The triangle is half the square
-// (76 MB at 6,162 items against 152 MB), so the scattered increments stay in L2.
-__global__ void k_pair_count(const int64_t* __restrict__ red_off, const int32_t* __restrict__ red_items, int64_t n_red,
-                             const int32_t* __restrict__ pos, int32_t nF, int32_t* __restrict__ T) {
+// (76 MB at 6,162 items against 152 MB), so the scattered increments stay in L2.  A thread
+// first gathers the row's positions in F into its own column of shared memory (at most
+// kPairRow; a longer row takes the direct loop) and sorts them, so each pair costs one
+// shared-memory read and one fire-and-forget add.
+__global__ void __launch_bounds__(kPairThreads) k_pair_count(const int64_t* __restrict__ red_off,
+                                                            const int32_t* __restrict__ red_items, int64_t n_red,
+                                                            const int32_t* __restrict__ pos, int32_t nF,
+                                                            int32_t* __restrict__ T) {
+    __shared__ int32_t buf[kPairRow * kPairThreads];
+    int32_t* my = buf + threadIdx.x;   // element k at my[k * kPairThreads]
     for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n_red; r += (int64_t)gridDim.x * blockDim.x) {
         const int64_t b = red_off[r], e = red_off[r + 1];
+        int n = 0;
+        bool spill = false;
+        for (int64_t x = b; x < e; x++) {
+            const int32_t p = __ldg(pos + __ldg(red_items + x));
+            if (p < 0) continue;
+            if (n == kPairRow) { spill = true; break; }
+            // insertion into the sorted column
+            int k = n++;
+            while (k > 0 && my[(k - 1) * kPairThreads] > p) {
+                my[k * kPairThreads] = my[(k - 1) * kPairThreads];
+                k--;
+            }
+            my[k * kPairThreads] = p;
+        }
+        if (!spill) {
+            for (int a = 0; a + 1 < n; a++) {
+                const int32_t i = my[a * kPairThreads];
+                int32_t* row = T + tri_row(i, nF);
+                for (int c = a + 1; c < n; c++) {
+                    const int32_t j = my[c * kPairThreads];
+                    if (j > i) atomicAdd(row + j, 1);
+                }
+            }
+            continue;
+        }
         for (int64_t x = b; x < e; x++) {
             const int32_t pa = __ldg(pos + red_items[x]);
             if (pa < 0) continue;
@@ -33,7 +70,7 @@ __global__ void k_pair_count(const int64_t* __restrict__ red_off, const int32_t*
                 const int32_t pb = __ldg(pos + red_items[y]);
                 if (pb < 0 || pb == pa) continue;
                 const int32_t i = min(pa, pb), j = max(pa, pb);
-                atomicAdd(T + tri_index(i, j, nF), 1);
+                atomicAdd(T + tri_row(i, nF) + j, 1);
             }
         }
     }
@@ -53,7 +90,7 @@ __global__ void __launch_bounds__(256) k_mirror_tri(const int32_t* __restrict__ 
         const int64_t r = (int64_t)bj * 32 + k, c = (int64_t)bi * 32 + tx;   // upper tile
         int32_t v = 0;
         if (r < nF && c < nF) {
-            if (r < c) v = T[tri_index((int32_t)r, (int32_t)c, nF)];
+            if (r < c) v = T[tri_row((int32_t)r, nF) + c];
             else if (r == c) v = diag ? diag[r] : 0;
             if (r <= c) M[r * nF + c] = v;
         }
@@ -98,9 +135,11 @@ int launch_pair_count(const int64_t* red_off, const int32_t* red_items, int64_t 
     int sms = 148, dev = 0;
     TFIM_CUDA(cudaGetDevice(&dev));
     TFIM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    int64_t blocks = (n_red + 255) / 256;
-    if (blocks > (int64_t)sms * 32) blocks = (int64_t)sms * 32;
-    k_pair_count<<<(unsigned)blocks, 256, 0, s>>>(red_off, red_items, n_red, pos, nF, T);
+    int per_sm = 0;
+    TFIM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_count, kPairThreads, 0));
+    int64_t blocks = (n_red + kPairThreads - 1) / kPairThreads;
+    if (blocks > (int64_t)sms * std::max(per_sm, 1)) blocks = (int64_t)sms * std::max(per_sm, 1);
+    k_pair_count<<<(unsigned)blocks, kPairThreads, 0, s>>>(red_off, red_items, n_red, pos, nF, T);
     TFIM_CUDA(cudaGetLastError());
     return TFIM_OK;
 }
