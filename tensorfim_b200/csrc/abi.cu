@@ -376,7 +376,7 @@ int tfim_mine(tfim_ctx* c, const tfim_mine_opts* opts, tfim_mine_stats* stats) {
     if (rc != TFIM_OK) return rc;
     st.device_ms = span_ms;
     st.host_ms = std::chrono::duration<double, std::milli>(t1 - t0).count() - st.sync_ms;
-    {
+    if (!c->mfis.ordered) {
         // descending support; ties by descending item lists (deterministic order)
         const MfiSet& M = c->mfis;
         auto before = [&](int32_t a, int32_t b) {
@@ -407,6 +407,7 @@ int tfim_mine(tfim_ctx* c, const tfim_mine_opts* opts, tfim_mine_stats* stats) {
         c->mfis.items.swap(S.items);
         c->mfis.off.swap(S.off);
         c->mfis.sup.swap(S.sup);
+        c->mfis.ordered = true;
     }
     st.n_mfi = (int64_t)c->mfis.size();
     // computation time as the reference reports it: search and counting, bitmap resident,

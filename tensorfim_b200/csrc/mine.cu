@@ -169,7 +169,7 @@ struct Wave {
 // host holds row_info (per global row: start,len) and the compacted entries.
 struct WaveRunner {
     tfim_ctx* c;
-    DevBuf d_desc, d_counts, d_entries, d_rowinfo, d_tri;
+    DevBuf d_desc, d_counts, d_entries, d_rowinfo;
     HostBuf h_desc, h_rowinfo, h_entries;
     std::vector<int2> row_info;
     std::vector<Entry> entries;
@@ -300,15 +300,7 @@ struct WaveRunner {
             return TFIM_OK;
         }
         TFIM_TRY(d_counts.reserve((size_t)std::max<int64_t>(w.out_total, 1) * 4));
-        if (w.top_job >= 0 && w.top_mode == 2) {
-            // the pair mirror writes every entry of the top block: zero only around it
-            const JobDesc& tj = w.jobs[w.top_job];
-            const int64_t t0 = tj.out_off, t1 = tj.out_off + (int64_t)tj.n_rows * tj.n_cols;
-            if (t0 > 0) TFIM_CUDA(cudaMemsetAsync(d_counts.p, 0, (size_t)t0 * 4, s));
-            if (w.out_total > t1) TFIM_CUDA(cudaMemsetAsync(d_counts.as<int32_t>() + t1, 0, (size_t)(w.out_total - t1) * 4, s));
-        } else {
-            TFIM_CUDA(cudaMemsetAsync(d_counts.p, 0, (size_t)w.out_total * 4, s));
-        }
+        TFIM_CUDA(cudaMemsetAsync(d_counts.p, 0, (size_t)w.out_total * 4, s));
         CountArgs a;
         a.bitmap = c->d_bitmap; a.W = W; a.masks = c->d_masks.as<uint32_t>();
         a.jobs = (const JobDesc*)(db + o_jobs); a.rows = (const RowDesc*)(db + o_rows);
@@ -317,13 +309,10 @@ struct WaveRunner {
             if (!ev[q]) TFIM_CUDA(cudaEventCreate(&ev[q]));
         const bool run_pairs = w.top_job >= 0 && w.top_mode == 2;
         TFIM_CUDA(cudaEventRecord(ev[0], s));
-        const int64_t tri = run_pairs ? pair_triangle_entries(w.jobs[w.top_job].n_rows) : 0;
         if (run_pairs) {
             const JobDesc& tj = w.jobs[w.top_job];
-            TFIM_TRY(d_tri.reserve((size_t)std::max<int64_t>(tri, 4) * 4));
-            TFIM_CUDA(cudaMemsetAsync(d_tri.p, 0, (size_t)tri * 4, s));
             TFIM_TRY(launch_pair_count(c->d_red_off, c->d_red_items, c->n_bits, (const int32_t*)(db + o_tpos), tj.n_rows,
-                                       d_tri.as<int32_t>(), s));
+                                       d_counts.as<int32_t>() + tj.out_off, s));
             launches++;
             count_launches++;
             path_launches[TFIM_PATH_PAIRS]++;
@@ -346,16 +335,11 @@ struct WaveRunner {
         }
         TFIM_CUDA(cudaEventRecord(ev[3], s));
         // a transaction-sharded context sums the partial counts of the whole wave over the group
-        // (the pair triangle too, before the mirror writes the whole-database diagonal)
         TFIM_TRY(group_reduce(c, d_counts.p, w.out_total, TFIM_DT_I32, TFIM_RED_SUM, s));
-        if (run_pairs) TFIM_TRY(group_reduce(c, d_tri.p, tri, TFIM_DT_I32, TFIM_RED_SUM, s));
         if (w.top_job >= 0) {
             const JobDesc& tj = w.jobs[w.top_job];
-            if (run_pairs)
-                TFIM_TRY(launch_mirror_tri(d_tri.as<int32_t>(), d_counts.as<int32_t>() + tj.out_off, tj.n_rows,
-                                           (const int32_t*)(db + o_tdiag), s));
-            else
-                TFIM_TRY(launch_mirror(d_counts.as<int32_t>() + tj.out_off, tj.n_rows, nullptr, s));
+            TFIM_TRY(launch_mirror(d_counts.as<int32_t>() + tj.out_off, tj.n_rows,
+                                   w.top_mode == 2 ? (const int32_t*)(db + o_tdiag) : nullptr, s));
             launches++;
         }
         if (want_full_counts) {
@@ -396,7 +380,7 @@ struct WaveRunner {
         return TFIM_OK;
     }
     void release() {
-        d_desc.release(); d_counts.release(); d_entries.release(); d_rowinfo.release(); d_tri.release();
+        d_desc.release(); d_counts.release(); d_entries.release(); d_rowinfo.release();
         h_desc.release(); h_rowinfo.release(); h_entries.release();
         for (cudaEvent_t& e : ev)
             if (e) {
@@ -483,8 +467,7 @@ void lookahead_features(float* f, int head_n, const std::vector<std::pair<int32_
 EngineState& engine_state(tfim_ctx* c) {
     if (!c->engine) {
         c->engine = new EngineState();
-        for (DevBuf* b : {&c->engine->wr.d_desc, &c->engine->wr.d_counts, &c->engine->wr.d_entries, &c->engine->wr.d_rowinfo,
-                          &c->engine->wr.d_tri})
+        for (DevBuf* b : {&c->engine->wr.d_desc, &c->engine->wr.d_counts, &c->engine->wr.d_entries, &c->engine->wr.d_rowinfo})
             b->stream = c->stream;
     }
     c->engine->wr.c = c;

@@ -1461,6 +1461,64 @@ __global__ void k_res_control(const ResArgs* __restrict__ args, cudaGraphConditi
     cudaGraphSetConditional(h, go ? 1u : 0u);
 }
 
+// ------------------------------------------------------------------------ output order
+// The MFIs leave the device in their output order: descending support, then item lists
+// (each in descending order) compared lexicographically, larger first.  The sort key packs
+// the support and the two largest items, complemented so that an ascending radix sort gives
+// that order.  Narrow keys (support below 2^24, item ids below 2^20 - 1) hold both items;
+// wide ones only the first.  Lists whose keys are equal are finished on the host.
+__global__ void __launch_bounds__(256) k_mfi_keys(const int32_t* __restrict__ off, const int32_t* __restrict__ len,
+                                                  const int32_t* __restrict__ sup, const int32_t* __restrict__ items,
+                                                  int32_t n, int wide, uint64_t* __restrict__ keys,
+                                                  int32_t* __restrict__ idx) {
+    for (int32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const int32_t o = off[k], l = len[k];
+        int32_t a = -1, b = -1;   // the two largest items
+        for (int32_t q = 0; q < l; q++) {
+            const int32_t x = items[o + q];
+            if (x > a) {
+                b = a;
+                a = x;
+            } else if (x > b) {
+                b = x;
+            }
+        }
+        const uint32_t s = (uint32_t)sup[k];
+        uint64_t key;
+        if (wide) key = ((uint64_t)(0xFFFFFFFFu - s) << 32) | (uint64_t)(0xFFFFFFFFu - (uint32_t)(a + 1));
+        else
+            key = ((uint64_t)(0xFFFFFFu - s) << 40) | ((uint64_t)(0xFFFFFu - (uint32_t)(a + 1)) << 20) |
+                  (uint64_t)(0xFFFFFu - (uint32_t)(b + 1));
+        keys[k] = key;
+        idx[k] = k;
+    }
+}
+
+// Lengths and supports in sorted order.
+__global__ void __launch_bounds__(256) k_mfi_permute(const int32_t* __restrict__ idx, const int32_t* __restrict__ len,
+                                                     const int32_t* __restrict__ sup, int32_t n,
+                                                     int32_t* __restrict__ len_o, int32_t* __restrict__ sup_o) {
+    for (int32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        const int32_t k = idx[q];
+        len_o[q] = len[k];
+        sup_o[q] = sup[k];
+    }
+}
+
+// Item lists in sorted order: one warp per MFI.
+__global__ void __launch_bounds__(256) k_mfi_gather(const int32_t* __restrict__ idx, const int32_t* __restrict__ off,
+                                                    const int32_t* __restrict__ items, const int32_t* __restrict__ off_o,
+                                                    const int32_t* __restrict__ len_o, int32_t n,
+                                                    int32_t* __restrict__ items_o) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t q = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); q < n; q += warps) {
+        const int32_t* src = items + off[idx[q]];
+        int32_t* dst = items_o + off_o[q];
+        for (int32_t x = lane; x < len_o[q]; x += 32) dst[x] = src[x];
+    }
+}
+
 // ---------------------------------------------------------------------------------- host
 struct Pool {
     void* p = nullptr;
@@ -1555,8 +1613,9 @@ int build_wave_graph(WaveGraph& G, const ResArgs* d_args, ResStatus* d_status, b
 
 struct ResidentState {
     Pool fams, items, heads, stack, looks, free_slots, defer, mfi_off, mfi_len, mfi_sup, mfi_items, log_feat, log_label;
-    Pool djobs, jobs, rows, row_job, row_local, tiles_l3, tiles_b1, tiles_tc, tiles_gr, counts, status, is_root, dense_freq, top_pos, top_tri,
+    Pool djobs, jobs, rows, row_job, row_local, tiles_l3, tiles_b1, tiles_tc, tiles_gr, counts, status, is_root, dense_freq, top_pos,
         top_diag, proj_list, args, top_sum, mjobs, sup_index;
+    Pool ord_keys, ord_idx, ord_meta, ord_items, ord_tmp;   // output order of the MFIs
     HostBuf h_status, h_args, h_res, h_setup;
     // the database's part of the search's initial state (root flags, the top family in
     // increasing support order), computed at a context's first resident mine and its pinned
@@ -1570,9 +1629,9 @@ struct ResidentState {
     void release(cudaStream_t s) {
         graph.release();
         for (Pool* b : {&fams, &items, &heads, &stack, &looks, &free_slots, &defer, &mfi_off, &mfi_len, &mfi_sup, &mfi_items,
-                        &log_feat, &log_label, &djobs, &jobs, &rows, &row_job, &row_local, &tiles_l3, &tiles_b1, &tiles_tc, &tiles_gr, &counts, &top_tri,
+                        &log_feat, &log_label, &djobs, &jobs, &rows, &row_job, &row_local, &tiles_l3, &tiles_b1, &tiles_tc, &tiles_gr, &counts,
                         &status, &is_root, &dense_freq, &top_pos, &top_diag, &proj_list, &args, &top_sum, &mjobs,
-                        &sup_index}) {
+                        &sup_index, &ord_keys, &ord_idx, &ord_meta, &ord_items, &ord_tmp}) {
             dev_free(b->p, s);
             b->p = nullptr;
             b->bytes = 0;
@@ -1653,6 +1712,87 @@ int release_cached(int dev) {
     }
     return TFIM_OK;
 }
+
+namespace {
+// Sorts the n MFIs of the pool (ni items) into output order on the device and queues the
+// copies of their sort keys (hkey[n]), lengths then supports (hmeta[2n]) and items
+// (hitems[ni]) into pinned host memory; they are valid once the stream has finished.
+int order_mfis(ResidentState& R, const tfim_ctx* c, const ResPtrs& P, int32_t n, int64_t ni, int sm_count,
+               cudaStream_t s, uint64_t* hkey, int32_t* hmeta, int32_t* hitems) {
+    int32_t max_sup = 0;
+    for (int32_t f : c->dense_freq) max_sup = std::max(max_sup, f);
+    const int wide = c->n_bits > 0xFFFFFF || max_sup > 0xFFFFFF || c->info.n_dense > 0xFFFFF ? 1 : 0;
+    size_t t_sort = 0, t_scan = 0;
+    TFIM_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, t_sort, (const uint64_t*)nullptr, (uint64_t*)nullptr,
+                                              (const int32_t*)nullptr, (int32_t*)nullptr, n, 0, 64, s));
+    TFIM_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, t_scan, (const int32_t*)nullptr, (int32_t*)nullptr, n, s));
+    TFIM_TRY(grow(R.ord_keys, (size_t)n * 16, s));
+    TFIM_TRY(grow(R.ord_idx, (size_t)n * 8, s));
+    TFIM_TRY(grow(R.ord_meta, ((size_t)n * 3 + 1) * 4, s));
+    TFIM_TRY(grow(R.ord_items, (size_t)std::max<int64_t>(ni, 1) * 4, s));
+    TFIM_TRY(grow(R.ord_tmp, std::max<size_t>(std::max(t_sort, t_scan), 16), s));
+    uint64_t* k_in = (uint64_t*)R.ord_keys.p;
+    uint64_t* k_out = k_in + n;
+    int32_t* i_in = (int32_t*)R.ord_idx.p;
+    int32_t* i_out = i_in + n;
+    int32_t* len_o = (int32_t*)R.ord_meta.p;
+    int32_t* sup_o = len_o + n;
+    int32_t* off_o = sup_o + n;
+    int32_t* items_o = (int32_t*)R.ord_items.p;
+    const unsigned grid = (unsigned)std::min<int64_t>(((int64_t)n + 255) / 256, (int64_t)sm_count * 8);
+    k_mfi_keys<<<grid, 256, 0, s>>>(P.mfi_off, P.mfi_len, P.mfi_sup, P.mfi_items, n, wide, k_in, i_in);
+    TFIM_CUDA(cudaGetLastError());
+    size_t t = R.ord_tmp.bytes;
+    TFIM_CUDA(cub::DeviceRadixSort::SortPairs(R.ord_tmp.p, t, k_in, k_out, i_in, i_out, n, 0, 64, s));
+    k_mfi_permute<<<grid, 256, 0, s>>>(i_out, P.mfi_len, P.mfi_sup, n, len_o, sup_o);
+    TFIM_CUDA(cudaGetLastError());
+    t = R.ord_tmp.bytes;
+    TFIM_CUDA(cub::DeviceScan::ExclusiveSum(R.ord_tmp.p, t, len_o, off_o, n, s));
+    const unsigned ggrid = (unsigned)std::min<int64_t>(((int64_t)n + 7) / 8, (int64_t)sm_count * 8);
+    k_mfi_gather<<<ggrid, 256, 0, s>>>(i_out, P.mfi_off, P.mfi_items, off_o, len_o, n, items_o);
+    TFIM_CUDA(cudaGetLastError());
+    TFIM_CUDA(cudaMemcpyAsync(hkey, k_out, (size_t)n * 8, cudaMemcpyDeviceToHost, s));
+    TFIM_CUDA(cudaMemcpyAsync(hmeta, len_o, (size_t)n * 8, cudaMemcpyDeviceToHost, s));   // len_o, sup_o
+    if (ni) TFIM_CUDA(cudaMemcpyAsync(hitems, items_o, (size_t)ni * 4, cudaMemcpyDeviceToHost, s));
+    return TFIM_OK;
+}
+
+// Finishes the output order on the host: item lists longer than 64 (the device sorts
+// shorter ones as it emits them) are sorted, then each run of equal sort keys is ordered by
+// the full comparison of item lists.
+void finish_mfi_order(MfiSet& M, const uint64_t* key) {
+    const size_t n = M.size();
+    for (size_t k = 0; k < n; k++)
+        if (M.off[k + 1] - M.off[k] > 64)
+            std::sort(M.items.begin() + M.off[k], M.items.begin() + M.off[k + 1], std::greater<int32_t>());
+    std::vector<int32_t> idx, items;
+    for (size_t a = 0; a < n;) {
+        size_t b = a + 1;
+        while (b < n && key[b] == key[a]) b++;
+        if (b - a > 1) {
+            idx.resize(b - a);
+            for (size_t q = a; q < b; q++) idx[q - a] = (int32_t)q;
+            std::sort(idx.begin(), idx.end(), [&](int32_t x, int32_t y) {
+                return std::lexicographical_compare(M.items.begin() + M.off[y], M.items.begin() + M.off[y + 1],
+                                                    M.items.begin() + M.off[x], M.items.begin() + M.off[x + 1]);
+            });
+            items.assign(M.items.begin() + M.off[a], M.items.begin() + M.off[b]);
+            const int64_t base = M.off[a];
+            int64_t o = base;
+            for (int32_t q : idx) {
+                const int64_t l = M.off[q + 1] - M.off[q];
+                std::copy(items.begin() + (M.off[q] - base), items.begin() + (M.off[q] - base) + l, M.items.begin() + o);
+                o += l;
+            }
+            // supports are equal within the run; the offsets follow the new lengths
+            std::vector<int64_t> lens(b - a);
+            for (size_t q = 0; q < idx.size(); q++) lens[q] = M.off[idx[q] + 1] - M.off[idx[q]];
+            for (size_t q = 0; q < idx.size(); q++) M.off[a + q + 1] = M.off[a + q] + lens[q];
+        }
+        a = b;
+    }
+}
+}  // namespace
 
 int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
     const auto t_entry = std::chrono::steady_clock::now();
@@ -2011,22 +2151,14 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
         if (!tl.empty())
             TFIM_CUDA(cudaMemcpyAsync(top_b1 ? R.tiles_b1.p : R.tiles_l3.p, tl.data(), tl.size() * sizeof(TileDesc),
                                       cudaMemcpyHostToDevice, s));
-        const int64_t tri = pair_triangle_entries(n0);
-        if (top_mode == 2) {
-            // pairs into the packed triangle; the mirror below writes every entry of the block
-            TFIM_TRY(grow(R.top_tri, (size_t)std::max<int64_t>(tri, 4) * 4, s));
-            TFIM_CUDA(cudaMemsetAsync(R.top_tri.p, 0, (size_t)tri * 4, s));
-        } else {
-            TFIM_CUDA(cudaMemsetAsync(R.counts.p, 0, (size_t)top_out * 4, s));
-        }
+        TFIM_CUDA(cudaMemsetAsync(R.counts.p, 0, (size_t)top_out * 4, s));
         CountArgs a;
         a.bitmap = c->d_bitmap; a.W = W; a.masks = c->d_masks.as<uint32_t>(); a.jobs = P.jobs; a.rows = P.rows;
         a.cols = P.items; a.out = P.counts;
         stt->setup_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_entry).count();
         TFIM_CUDA(cudaEventRecord(c->ev0, s));
         if (top_mode == 2) {
-            TFIM_TRY(launch_pair_count(c->d_red_off, c->d_red_items, c->n_bits, (const int32_t*)R.top_pos.p, n0,
-                                       (int32_t*)R.top_tri.p, s));
+            TFIM_TRY(launch_pair_count(c->d_red_off, c->d_red_items, c->n_bits, (const int32_t*)R.top_pos.p, n0, P.counts, s));
             bytes_alg += (c->n_bits + 1) * 8 + c->n_red_items * 4 + 4 * top_out;
         } else {
             a.tiles = top_b1 ? P.tiles_b1 : P.tiles_l3;
@@ -2035,8 +2167,7 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
             bytes_alg += row_bytes * 2 * n0 + 4 * top_out;
         }
         TFIM_CUDA(cudaEventRecord(c->ev1, s));
-        if (top_mode == 2) TFIM_TRY(launch_mirror_tri((const int32_t*)R.top_tri.p, P.counts, n0, (const int32_t*)R.top_diag.p, s));
-        else TFIM_TRY(launch_mirror(P.counts, n0, nullptr, s));
+        TFIM_TRY(launch_mirror(P.counts, n0, top_mode == 2 ? (const int32_t*)R.top_diag.p : nullptr, s));
         TFIM_TRY(grow(R.top_sum, (size_t)n0 * sizeof(RowSum), s));
         k_top_summary<<<n0, 256, 0, s>>>(P.counts, n0, minc, (RowSum*)R.top_sum.p);
         TFIM_CUDA(cudaGetLastError());
@@ -2203,18 +2334,18 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
     // results
     const auto t_read0 = std::chrono::steady_clock::now();
     const ResStatus fin = *hst;
-    // the MFI pool through one pinned staging buffer: offsets, lengths, supports, items
-    const size_t nm = (size_t)fin.mfi_n, ni = (size_t)fin.mfi_item_n;
-    TFIM_TRY(R.h_res.reserve((3 * nm + ni + 1) * 4));
-    int32_t* moff = R.h_res.as<int32_t>();
-    int32_t* mlen = moff + nm;
-    int32_t* msup = mlen + nm;
-    int32_t* mitems = msup + nm;
+    // the MFIs in output order (sorted on the device) through one pinned staging buffer:
+    // sort keys, lengths, supports, items
+    const int32_t nm = fin.mfi_n;
+    const int64_t ni = fin.mfi_item_n;
+    TFIM_TRY(R.h_res.reserve(((size_t)nm * 4 + (size_t)ni + 2) * 4));
+    uint64_t* hkey = R.h_res.as<uint64_t>();
+    int32_t* hlen = (int32_t*)(hkey + nm);
+    int32_t* hsup = hlen + nm;
+    int32_t* hitems = hsup + nm;
     if (nm) {
-        TFIM_CUDA(cudaMemcpyAsync(moff, R.mfi_off.p, nm * 4, cudaMemcpyDeviceToHost, s));
-        TFIM_CUDA(cudaMemcpyAsync(mlen, R.mfi_len.p, nm * 4, cudaMemcpyDeviceToHost, s));
-        TFIM_CUDA(cudaMemcpyAsync(msup, R.mfi_sup.p, nm * 4, cudaMemcpyDeviceToHost, s));
-        TFIM_CUDA(cudaMemcpyAsync(mitems, R.mfi_items.p, ni * 4, cudaMemcpyDeviceToHost, s));
+        refresh_ptrs();
+        TFIM_TRY(order_mfis(R, c, P, nm, ni, sm_count, s, hkey, hlen, hitems));
     }
     if (o->log_lookahead && fin.log_n) {
         c->la_feats.resize((size_t)fin.log_n * 32);
@@ -2227,21 +2358,22 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
     if (used_tc) TFIM_TRY(count_fam_status(true));
     {
         MfiSet& M = c->mfis;
-        const size_t base = M.items.size();
-        M.items.resize(base + (size_t)fin.mfi_item_n);
-        M.off.reserve(M.off.size() + (size_t)fin.mfi_n);
-        M.sup.reserve(M.sup.size() + (size_t)fin.mfi_n);
-        size_t o = base;
-        for (int32_t k = 0; k < fin.mfi_n; k++) {
-            int32_t* dst = M.items.data() + o;
-            std::copy(mitems + moff[k], mitems + moff[k] + mlen[k], dst);
-            if (!std::is_sorted(dst, dst + mlen[k], std::greater<int32_t>()))   // lists over 64 items
-                std::sort(dst, dst + mlen[k], std::greater<int32_t>());
-            o += (size_t)mlen[k];
-            M.off.push_back((int64_t)o);
-            M.sup.push_back(msup[k]);
+        const bool fresh = M.size() == 0;
+        const size_t kbase = M.size();
+        M.items.insert(M.items.end(), hitems, hitems + ni);
+        M.sup.insert(M.sup.end(), hsup, hsup + nm);
+        M.off.resize(kbase + 1 + (size_t)nm);
+        for (int32_t k = 0; k < nm; k++) M.off[kbase + k + 1] = M.off[kbase + k] + hlen[k];
+        if (fresh) {
+            finish_mfi_order(M, hkey);
+            M.ordered = true;
+        } else {
+            // appended to earlier results: long lists sorted here, the whole set by the caller
+            for (size_t k = kbase; k < M.size(); k++)
+                if (M.off[k + 1] - M.off[k] > 64)
+                    std::sort(M.items.begin() + M.off[k], M.items.begin() + M.off[k + 1], std::greater<int32_t>());
+            M.ordered = false;
         }
-        M.items.resize(o);
     }
     stt->nodes += (int64_t)fin.nodes;
     stt->supports += (int64_t)fin.supports;

@@ -197,11 +197,6 @@ int occupancy_gram(int* blocks);
 int configure_gram_kernel();
 // The tuning table in force (common.cu): built-in values, or the table loaded / set.
 tfim_tuning tuning();
-// Pair co-occurrence of the empty-prefix family into the packed upper triangle T
-// (pair_triangle_entries(nF) int32 entries, zeroed by the caller); launch_mirror_tri writes
-// every entry of the full nF x nF matrix from it (the diagonal from diag, or zero).
-int64_t pair_triangle_entries(int32_t nF);
-int launch_mirror_tri(const int32_t* T, int32_t* M, int32_t nF, const int32_t* diag, cudaStream_t s);
 int launch_pair_count(const int64_t* red_off, const int32_t* red_items, int64_t n_red, const int32_t* pos,
                       int32_t nF, int32_t* M, cudaStream_t s);
 int launch_mirror(int32_t* M, int32_t nF, const int32_t* diag, cudaStream_t s);
@@ -232,11 +227,13 @@ struct MfiSet {
     std::vector<int32_t> items;
     std::vector<int64_t> off{0};
     std::vector<int32_t> sup;
+    bool ordered = false;   // already in output order (descending support, then item lists)
     size_t size() const { return sup.size(); }
     void clear() {
         items.clear();
         off.assign(1, 0);
         sup.clear();
+        ordered = false;
     }
     void add(const int32_t* x, size_t n, int32_t s) {
         items.insert(items.end(), x, x + n);

@@ -231,3 +231,43 @@ def test_dense_families_take_the_gram_and_tensor_paths(tmp_path, graphs):
         b = db.mine(engine="resident", counter="lop3", graphs=graphs)
         assert b.as_dict() == fx["expected"]
         assert b.stats["path_supports"][gram] == 0 and b.stats["path_supports"][tc] == 0
+
+
+def _long_and_tied_db():
+    """150 rows of items 0..69 (an MFI longer than the device sorts per warp), and two blocks
+    of ten MFIs {a, b, x_k} of support 10 whose shared items a, b are the two largest in one
+    block under an ascending-frequency item order and in the other under a descending one,
+    so that MFIs with equal support and equal two largest items occur either way."""
+    rows = [list(range(70))] * 150
+    for k in range(10):
+        rows += [[199, 200, 201 + k]] * 10          # 199, 200: support 100; 201+k: 10
+        rows += [[400, 401, 410 + k]] * 10          # 400, 401: support 100
+        rows += [[410 + k]] * 100                   # 410+k: support 110
+    off = np.zeros(len(rows) + 1, np.int64)
+    off[1:] = np.cumsum([len(x) for x in rows])
+    return off, np.concatenate([np.asarray(x, np.int32) for x in rows])
+
+
+@pytest.mark.parametrize("name", ["cfg1_full", "cfg4_s001", "edge_ties", "cfg3_base", "long_tied"])
+def test_resident_output_order_equals_the_host_order(tmp_path, name):
+    """The resident engine sorts its MFIs on the device (support, then the two largest items)
+    and finishes equal keys on the host; the batched engine sorts on the host.  Both give
+    one sequence: descending support, then item lists in descending order."""
+    if name == "long_tied":
+        off, items = _long_and_tied_db()
+        db = tf.Database.from_csr(off, items, 0.007)   # 10 of 1,350 rows
+    else:
+        fx = load_golden(name)
+        db = tf.Database.from_file(golden_input(fx, tmp_path), fx["spec"]["minsup"])
+    la = "all" if name == "long_tied" else True   # the 70-item set is found by its lookahead
+    with db:
+        host = db.mine(engine="batched", lookahead=la).mfis
+        for v in (dict(), dict(graphs=True), dict(counter="lop3", top="bitmap")):
+            got = db.mine(engine="resident", lookahead=la, **v).mfis
+            assert got == host, v
+    sups = [s for _, s in host]
+    assert sups == sorted(sups, reverse=True)
+    if name == "long_tied":
+        assert len(host) == 21 and max(len(x) for x, _ in host) == 70
+        keys = [(s, x[:2]) for x, s in host]
+        assert len(set(keys)) < len(keys)   # equal device keys were finished on the host
