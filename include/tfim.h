@@ -150,9 +150,9 @@ TFIM_API int tfim_open_bitmap_sharded(const uint32_t* rows, int32_t n_rows, int6
                                       int32_t device, const tfim_group* group, tfim_ctx** out);
 
 TFIM_API int tfim_db_info_get(const tfim_ctx* ctx, tfim_db_info* out);
-/* dense id -> original id (n_dense entries) */
+/* dense id -> original id (n_dense entries; out may be null when there are none) */
 TFIM_API int tfim_dense_to_orig(const tfim_ctx* ctx, int32_t* out);
-/* occurrence count per dense id (n_dense entries) */
+/* occurrence count per dense id (n_dense entries; out may be null when there are none) */
 TFIM_API int tfim_dense_freq(const tfim_ctx* ctx, int32_t* out);
 
 /*

@@ -262,13 +262,14 @@ int tfim_db_info_get(const tfim_ctx* c, tfim_db_info* out) {
 }
 
 int tfim_dense_to_orig(const tfim_ctx* c, int32_t* out) {
-    TFIM_CHECK(c && out, TFIM_E_INVALID, "null argument");
+    TFIM_CHECK(c && (out || c->dense_to_orig.empty()), TFIM_E_INVALID, "null argument");
     std::copy(c->dense_to_orig.begin(), c->dense_to_orig.end(), out);
     return TFIM_OK;
 }
 
 int tfim_dense_freq(const tfim_ctx* c, int32_t* out) {
-    TFIM_CHECK(c && out, TFIM_E_INVALID, "null argument");
+    TFIM_CHECK(c && (out || (c->from_db ? c->dense_freq.empty() : c->bit_support.empty())), TFIM_E_INVALID,
+               "null argument");
     if (c->from_db) std::copy(c->dense_freq.begin(), c->dense_freq.end(), out);
     else std::copy(c->bit_support.begin(), c->bit_support.end(), out);
     return TFIM_OK;

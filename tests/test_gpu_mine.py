@@ -263,7 +263,7 @@ def _output_order(db, mfis):
     return [(tuple(int(d2o[-x]) for x in t[1]), t[4]) for t in keyed]
 
 
-@pytest.mark.parametrize("name", ["cfg1_full", "cfg4_s001", "edge_ties", "cfg3_base", "long_tied"])
+@pytest.mark.parametrize("name", ["cfg1_full", "cfg4_s001", "edge_ties", "cfg3_base", "cfg3_base_t06", "long_tied"])
 def test_resident_output_order(tmp_path, name):
     """The resident engine sorts its MFIs on the device (support, then the two largest items)
     and finishes equal keys on the host; the batched engine sorts on the host.  Both give the
