@@ -234,11 +234,12 @@ def test_dense_families_take_the_gram_and_tensor_paths(tmp_path, graphs):
 
 
 def _long_and_tied_db():
-    """150 rows of items 0..69 (an MFI longer than the device sorts per warp), and two blocks
+    """150 rows of items 1..70 (an MFI longer than the device sorts per warp; id 0, which the
+    reference searches apart with lists of at most 64 items, is left out), and two blocks
     of ten MFIs {a, b, x_k} of support 10 whose shared items a, b are the two largest in one
     block under an ascending-frequency item order and in the other under a descending one,
     so that MFIs with equal support and equal two largest items occur either way."""
-    rows = [list(range(70))] * 150
+    rows = [list(range(1, 71))] * 150
     for k in range(10):
         rows += [[199, 200, 201 + k]] * 10          # 199, 200: support 100; 201+k: 10
         rows += [[400, 401, 410 + k]] * 10          # 400, 401: support 100
