@@ -90,23 +90,37 @@ __device__ void lop3_tile_impl(const CountArgs& a, const TileDesc t, Lop3Shared&
     const int wcap = min(kL3Pos / 8, (kL3Stage / 8) / nr);
     int ns = 0;   // staged positions of this warp (warp-uniform)
 
+    // U staged positions per lane and pass: their column words are all requested before the
+    // first is used, so a thin tile (one or two rows, each column word feeding one or two
+    // popcounts) keeps several L2 reads in flight per lane instead of one.
+    constexpr int U = WIDE ? 2 : 4;
     auto flush = [&]() {
         __syncwarp();
-        for (int k0 = 0; k0 < ns; k0 += G) {
-            const int k = k0 + koff;
-            if (!active || k >= ns) continue;
-            const int p = wpos[k];
-            uint4 v[NC];
+        for (int k0 = 0; k0 < ns; k0 += G * U) {
+            uint4 v[U][NC];
+            int kk[U];
 #pragma unroll
-            for (int ci = 0; ci < NC; ci++)
-                v[ci] = ck[ci] == 0 ? __ldg(cp[ci] + p) : ck[ci] == 1 ? make_uint4(~0u, ~0u, ~0u, ~0u) : make_uint4(0, 0, 0, 0);
-            const uint4* st = wst + k * nr;
+            for (int u = 0; u < U; u++) {
+                const int k = k0 + u * G + koff;
+                kk[u] = active && k < ns ? k : -1;
+                const int p = kk[u] >= 0 ? wpos[k] : 0;
 #pragma unroll
-            for (int r = 0; r < kLop3Rows; r++) {
-                if (r >= nr) break;
-                const uint4 m = st[r];
+                for (int ci = 0; ci < NC; ci++)
+                    v[u][ci] = kk[u] < 0 || ck[ci] == 2 ? make_uint4(0, 0, 0, 0)
+                               : ck[ci] == 0         ? __ldg(cp[ci] + p)
+                                                     : make_uint4(~0u, ~0u, ~0u, ~0u);
+            }
 #pragma unroll
-                for (int ci = 0; ci < NC; ci++) acc[ci][r] += popc4(and4(m, v[ci]));
+            for (int u = 0; u < U; u++) {
+                if (kk[u] < 0) continue;
+                const uint4* st = wst + kk[u] * nr;
+#pragma unroll
+                for (int r = 0; r < kLop3Rows; r++) {
+                    if (r >= nr) break;
+                    const uint4 m = st[r];
+#pragma unroll
+                    for (int ci = 0; ci < NC; ci++) acc[ci][r] += popc4(and4(m, v[u][ci]));
+                }
             }
         }
         __syncwarp();
