@@ -36,7 +36,7 @@ extern "C" {
 #define TFIM_E_DEPTH       4   /* an item list longer than the counter supports */
 #define TFIM_E_TIMEOUT     5   /* a bounded device-side wait expired */
 #define TFIM_E_STATE       6   /* call order violated (e.g. results before tfim_mine) */
-#define TFIM_E_IO          7   /* results file could not be written */
+#define TFIM_E_IO          7   /* a transaction file could not be read, or a results file written */
 #define TFIM_E_COMM        8   /* a sharded context's all-reduce callback reported failure */
 
 typedef struct tfim_ctx tfim_ctx;
@@ -89,6 +89,33 @@ typedef struct {
  */
 TFIM_API int tfim_open_db(const int64_t* row_offsets, const int32_t* items, int64_t n_rows,
                  double support_threshold, int32_t device, tfim_ctx** out);
+
+/*
+ * Build the device database from the bytes of a transaction file, parsed on the GPU.
+ * The bytes are copied to device memory (in chunks through pinned staging, or in one copy
+ * from a pinned buffer) and two passes over them produce the CSR that tfim_open_db takes,
+ * with the reference's parse rules: every '\n' ends a row (empty rows included), a maximal
+ * run of digits is an id, a run right after '-' is dropped, every other byte separates,
+ * and a last row without '\n' counts only when it holds an id.  Ingest then continues as in
+ * tfim_open_db.  Ids accumulate modulo 2^32 (the reference's value for runs of up to 18
+ * digits); an id above INT32_MAX reads as negative and is rejected (TFIM_E_INVALID).
+ *
+ * Replaces readTransSetFile (code/engine/src/kernel_bitmap.cu:205-267) and its successors.
+ */
+TFIM_API int tfim_open_text(const char* bytes, int64_t n_bytes, double support_threshold, int32_t device,
+                            tfim_ctx** out);
+/* tfim_open_text over a file's contents, read with worker threads straight into the pinned
+ * staging (TFIM_E_IO when it cannot be opened or read).  Used by the `tfim` command. */
+TFIM_API int tfim_open_file(const char* path, double support_threshold, int32_t device, tfim_ctx** out);
+/*
+ * The parse alone: the CSR of a transaction file's bytes, built on `device` and copied to
+ * the caller's arrays.  Always sets *n_rows and *n_items; with null row_offsets and items
+ * it only measures, and with arrays smaller than n_rows + 1 offsets or n_items ids it
+ * returns TFIM_E_NOMEM and writes neither.  Replaces readTransSetFile's scanner
+ * (code/engine/src/kernel_bitmap.cu:205-233) for callers that keep their own ingest.
+ */
+TFIM_API int tfim_parse_text(const char* bytes, int64_t n_bytes, int32_t device, int64_t* row_offsets, int64_t rows_cap,
+                             int32_t* items, int64_t items_cap, int64_t* n_rows, int64_t* n_items);
 
 /*
  * Open a context over a vertical bitmap supplied directly: n_rows rows of

@@ -75,6 +75,7 @@ def lib() -> C.CDLL:
             getattr(L, name).argtypes = [p, p]
         L.tfo_write_results.argtypes = [p, C.c_char_p, C.c_char_p]
         L.tfo_count_wave.argtypes = [p, i64, p, p, i32, i32, i32, p, p]
+        L.tfo_parse.argtypes = [C.c_char_p, C.POINTER(i64), C.POINTER(i64), p, i64, p, i64]
         _lib = L
     return _lib
 
@@ -159,6 +160,18 @@ def mine_file(path: str, minsup: float, threads: int = 0) -> dict:
         return db.mine(threads)
     finally:
         db.close()
+
+
+def parse_file(path: str) -> tuple[np.ndarray, np.ndarray]:
+    """The oracle's parse of a transaction file as CSR (offsets int64, items int32)."""
+    L = lib()
+    rows, n = C.c_int64(), C.c_int64()
+    if L.tfo_parse(path.encode(), C.byref(rows), C.byref(n), None, 0, None, 0) != 0:
+        raise FileNotFoundError(path)
+    off = np.zeros(rows.value + 1, np.int64)
+    items = np.zeros(max(n.value, 1), np.int32)
+    L.tfo_parse(path.encode(), C.byref(rows), C.byref(n), _p(off), off.size, _p(items), items.size)
+    return off, items[:n.value]
 
 
 def count_wave(rows: np.ndarray, lists: list, d: int, min_count: int) -> tuple[np.ndarray, np.ndarray]:

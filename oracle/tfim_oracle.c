@@ -388,6 +388,22 @@ TFO_API int64_t tfo_mine_sample(tfo_db* db, double budget_s, int nthreads, doubl
 }
 
 /* ------------------------------------------------------------------ accessors */
+/* The parse alone (kernel_bitmap.cu:205-233): sets *nRows and *nItems; fills off (nRows + 1)
+ * and items when both are given and large enough.  Returns -1 when the file cannot be read. */
+TFO_API int tfo_parse(const char* path, int64_t* nRows, int64_t* nItems, int64_t* off, int64_t offCap, int32_t* items,
+                      int64_t itemsCap) {
+    ivec it = {0}; lvec rs = {0};
+    if (parse_file(path, &it, &rs) != 0) { free(it.v); free(rs.v); return -1; }
+    *nRows = rs.n - 1;
+    *nItems = it.n;
+    if (off && items && offCap >= rs.n && itemsCap >= it.n) {
+        memcpy(off, rs.v, (size_t)rs.n * 8);
+        if (it.n) memcpy(items, it.v, (size_t)it.n * 4);
+    }
+    free(it.v); free(rs.v);
+    return 0;
+}
+
 TFO_API int64_t tfo_num_mfis(const tfo_db* db) { return db->nMfi; }
 TFO_API int64_t tfo_nodes_visited(const tfo_db* db) { return db->nodesVisited; }
 TFO_API double tfo_comp_time(const tfo_db* db) { return db->compTime; }

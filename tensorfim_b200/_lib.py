@@ -47,6 +47,7 @@ EXPORTS = [
     "tfim_mlp_grad", "tfim_mlp_train", "tfim_mlp_free", "tfim_set_proposal", "tfim_lookahead_log",
     "tfim_tuning_get", "tfim_tuning_set", "tfim_tuning_load", "tfim_tuning_source",
     "tfim_mine_all", "tfim_num_all", "tfim_all_item_total", "tfim_get_all", "tfim_release_cached",
+    "tfim_open_text", "tfim_open_file", "tfim_parse_text",
 ]
 
 
@@ -140,6 +141,9 @@ def lib() -> C.CDLL:
     L.tfim_last_error.restype = C.c_char_p
     L.tfim_open_db.argtypes = [p, p, i64, C.c_double, i32, P(p)]
     L.tfim_open_bitmap.argtypes = [p, i32, i64, i32, i32, P(p)]
+    L.tfim_open_text.argtypes = [p, i64, C.c_double, i32, P(p)]
+    L.tfim_open_file.argtypes = [C.c_char_p, C.c_double, i32, P(p)]
+    L.tfim_parse_text.argtypes = [p, i64, i32, p, i64, p, i64, P(i64), P(i64)]
     L.tfim_db_info_get.argtypes = [p, P(DbInfo)]
     L.tfim_dense_to_orig.argtypes = [p, p]
     L.tfim_dense_freq.argtypes = [p, p]

@@ -24,7 +24,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", *ARCH, "-Xcompiler", "-fPIC,-fvisibility=hidden",
            "-I" + INCLUDE, "-I" + CSRC, "-diag-suppress", "177"]
 
-CU_SOURCES = ["common.cu", "ingest.cu", "count_lop3.cu", "count_b1.cu", "count_pairs.cu", "count_proj.cu", "count_tc.cu", "count_fam.cu", "count_gram.cu", "allfi.cu", "shard.cu", "count_static.cu", "mlp.cu", "mine.cu", "resident.cu", "abi.cu"]
+CU_SOURCES = ["common.cu", "parse.cu", "ingest.cu", "count_lop3.cu", "count_b1.cu", "count_pairs.cu", "count_proj.cu", "count_tc.cu", "count_fam.cu", "count_gram.cu", "allfi.cu", "shard.cu", "count_static.cu", "mlp.cu", "mine.cu", "resident.cu", "abi.cu"]
 HEADERS = [os.path.join(CSRC, "tfim_internal.h"), os.path.join(INCLUDE, "tfim.h")]
 
 

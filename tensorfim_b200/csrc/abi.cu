@@ -1,4 +1,6 @@
 // extern "C" entry points of libtfim (declared in include/tfim.h).
+#include <fcntl.h>
+#include <sys/stat.h>
 #include <unistd.h>
 
 #include <algorithm>
@@ -215,6 +217,102 @@ int tfim_open_db(const int64_t* row_offsets, const int32_t* items, int64_t n_row
     if (rc != TFIM_OK) { tfim_close(c); return rc; }
     *out = c;
     return TFIM_OK;
+}
+
+}  // extern "C"
+
+namespace {
+int open_from_text(const TextSource& src, double thr, int32_t device, tfim_ctx** out) {
+    TFIM_CHECK(out != nullptr, TFIM_E_INVALID, "null output handle");
+    *out = nullptr;
+    TFIM_CHECK(thr > 0.0 && thr <= 1.0 && std::isfinite(thr), TFIM_E_INVALID, "support threshold %g outside (0, 1]", thr);
+    tfim_ctx* c = nullptr;
+    TFIM_TRY(make_ctx(device, &c));
+    int64_t* d_off = nullptr;
+    int32_t* d_items = nullptr;
+    int64_t n_rows = 0, nnz = 0;
+    int rc = parse_text_device(src, c->stream, &d_off, &d_items, &n_rows, &nnz);
+    if (rc == TFIM_OK) rc = ingest_device_csr(c, d_off, d_items, n_rows, nnz, thr);
+    dev_free(d_off, c->stream);
+    dev_free(d_items, c->stream);
+    if (rc != TFIM_OK) { tfim_close(c); return rc; }
+    *out = c;
+    return TFIM_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int tfim_open_text(const char* bytes, int64_t n_bytes, double support_threshold, int32_t device, tfim_ctx** out) {
+    TFIM_CHECK(n_bytes >= 0 && (bytes != nullptr || n_bytes == 0), TFIM_E_INVALID, "invalid transaction file bytes");
+    TextSource src;
+    src.host = bytes ? bytes : "";
+    src.n_bytes = n_bytes;
+    return open_from_text(src, support_threshold, device, out);
+}
+
+int tfim_open_file(const char* path, double support_threshold, int32_t device, tfim_ctx** out) {
+    TFIM_CHECK(out != nullptr, TFIM_E_INVALID, "null output handle");
+    *out = nullptr;
+    TFIM_CHECK(path != nullptr, TFIM_E_INVALID, "null path");
+    const int fd = open(path, O_RDONLY | O_CLOEXEC);
+    TFIM_CHECK(fd >= 0, TFIM_E_IO, "%s open failed", path);
+    struct stat st{};
+    if (fstat(fd, &st) != 0 || !S_ISREG(st.st_mode)) {
+        close(fd);
+        set_error("%s is not a readable regular file", path);
+        return TFIM_E_IO;
+    }
+    TextSource src;
+    src.fd = fd;
+    src.n_bytes = (int64_t)st.st_size;
+    const int rc = open_from_text(src, support_threshold, device, out);
+    close(fd);
+    return rc;
+}
+
+int tfim_parse_text(const char* bytes, int64_t n_bytes, int32_t device, int64_t* row_offsets, int64_t rows_cap,
+                    int32_t* items, int64_t items_cap, int64_t* n_rows, int64_t* n_items) {
+    TFIM_CHECK(n_bytes >= 0 && (bytes != nullptr || n_bytes == 0) && n_rows && n_items, TFIM_E_INVALID,
+               "tfim_parse_text: invalid arguments");
+    int n_dev = 0;
+    if (cudaGetDeviceCount(&n_dev) != cudaSuccess || n_dev <= 0) {
+        cudaGetLastError();
+        set_error("no CUDA device available");
+        return TFIM_E_CUDA;
+    }
+    TFIM_CHECK(device >= 0 && device < n_dev, TFIM_E_INVALID, "device %d out of range (%d devices)", device, n_dev);
+    TFIM_CUDA(cudaSetDevice(device));
+    cudaStream_t s = nullptr;
+    TFIM_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    TextSource src;
+    src.host = bytes ? bytes : "";
+    src.n_bytes = n_bytes;
+    int64_t* d_off = nullptr;
+    int32_t* d_items = nullptr;
+    int64_t rows = 0, nnz = 0;
+    int rc = parse_text_device(src, s, &d_off, &d_items, &rows, &nnz);
+    if (rc == TFIM_OK) {
+        *n_rows = rows;
+        *n_items = nnz;
+        if (row_offsets && items && rows_cap >= rows + 1 && items_cap >= nnz) {
+            if (cudaMemcpyAsync(row_offsets, d_off, (size_t)(rows + 1) * 8, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+                (nnz > 0 && cudaMemcpyAsync(items, d_items, (size_t)nnz * 4, cudaMemcpyDeviceToHost, s) != cudaSuccess) ||
+                cudaStreamSynchronize(s) != cudaSuccess) {
+                set_error("device-to-host copy of the parsed transactions failed");
+                rc = TFIM_E_CUDA;
+            }
+        } else if (row_offsets || items) {
+            set_error("tfim_parse_text: output capacity too small (%lld rows + 1, %lld items needed)", (long long)rows,
+                      (long long)nnz);
+            rc = TFIM_E_NOMEM;
+        }
+    }
+    dev_free(d_off, s);
+    dev_free(d_items, s);
+    cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+    return rc;
 }
 
 int tfim_open_bitmap(const uint32_t* rows, int32_t n_rows, int64_t n_bits, int32_t n_counted, int32_t device,

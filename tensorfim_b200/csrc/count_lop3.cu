@@ -72,10 +72,11 @@ __device__ void lop3_tile_impl(const CountArgs& a, const TileDesc t, Lop3Shared&
         ck[ci] = 2;
         cp[ci] = nullptr;
         if (cl[ci] >= 0 && cl[ci] < ncols && active) {
-            if (c == j.self_col) ck[ci] = 1;
+            const int32_t col = c == j.self_col ? -1 : a.cols[j.col_off + c];
+            if (col < 0) ck[ci] = 1;   // the all-ones column
             else {
                 ck[ci] = 0;
-                cp[ci] = reinterpret_cast<const uint4*>(a.bitmap + (int64_t)a.cols[j.col_off + c] * W);
+                cp[ci] = reinterpret_cast<const uint4*>(a.bitmap + (int64_t)col * W);
             }
         }
     }

@@ -171,10 +171,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_count_i8(CountArgs a) {
         col_src[c] = nullptr;
         col_kind[c] = 2;
         if (t.c0 + c < t.c1) {
-            if (t.c0 + c == j.self_col) col_kind[c] = 1;
+            const int32_t col = t.c0 + c == j.self_col ? -1 : a.cols[j.col_off + t.c0 + c];
+            if (col < 0) col_kind[c] = 1;   // the all-ones column
             else {
                 col_kind[c] = 0;
-                col_src[c] = a.bitmap + (int64_t)a.cols[j.col_off + t.c0 + c] * W;
+                col_src[c] = a.bitmap + (int64_t)col * W;
             }
         }
     }

@@ -258,31 +258,43 @@ int ingest_csr(tfim_ctx* c, const int64_t* h_off, const int32_t* h_items, int64_
     TFIM_CHECK(base == 0, TFIM_E_INVALID, "row_offsets[0] must be 0");
     const int64_t nnz = n_rows > 0 ? h_off[n_rows] : 0;
     TFIM_CHECK(nnz >= 0, TFIM_E_INVALID, "row_offsets[n_rows] is negative");
+    DevBuf d_off, d_items;
+    d_off.stream = d_items.stream = s;
+    int rc = TFIM_OK;
+    if (!(rc = d_off.reserve((size_t)(n_rows + 1) * 8)) && !(rc = d_items.reserve((size_t)std::max<int64_t>(nnz, 1) * 4))) {
+        if (cudaMemcpyAsync(d_off.p, h_off, (size_t)(n_rows + 1) * 8, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+            (nnz > 0 && cudaMemcpyAsync(d_items.p, h_items, (size_t)nnz * 4, cudaMemcpyHostToDevice, s) != cudaSuccess)) {
+            set_error("host-to-device copy of the transaction set failed");
+            rc = TFIM_E_CUDA;
+        } else {
+            rc = ingest_device_csr(c, d_off.as<int64_t>(), d_items.as<int32_t>(), n_rows, nnz, thr);
+        }
+    }
+    d_off.release();
+    d_items.release();
+    return rc;
+}
 
-    DevBuf d_off, d_items, d_stats, d_freq, d_map, d_flag, d_idx, d_tmp;
-    for (DevBuf* b : {&d_off, &d_items, &d_stats, &d_freq, &d_map, &d_flag, &d_idx, &d_tmp}) b->stream = s;
+int ingest_device_csr(tfim_ctx* c, const int64_t* d_off_p, const int32_t* d_items_p, int64_t n_rows, int64_t nnz,
+                      double thr) {
+    cudaStream_t s = c->stream;
+    DevBuf d_stats, d_freq, d_map, d_flag, d_idx, d_tmp;
+    for (DevBuf* b : {&d_stats, &d_freq, &d_map, &d_flag, &d_idx, &d_tmp}) b->stream = s;
     int rc = TFIM_OK;
     ScanStats hs{};
     std::vector<int32_t> freq;
     int64_t id_max = 0, id_min = INT_MAX;
     // all device scratch below is released at the end of this function
     auto done = [&](int r) {
-        d_off.release(); d_items.release(); d_stats.release(); d_freq.release();
+        d_stats.release(); d_freq.release();
         d_map.release(); d_flag.release(); d_idx.release(); d_tmp.release();
         return r;
     };
-    if ((rc = d_off.reserve((size_t)(n_rows + 1) * 8)) || (rc = d_items.reserve((size_t)std::max<int64_t>(nnz, 1) * 4)) ||
-        (rc = d_stats.reserve(sizeof(ScanStats))))
-        return done(rc);
-    if (cudaMemcpyAsync(d_off.p, h_off, (size_t)(n_rows + 1) * 8, cudaMemcpyHostToDevice, s) != cudaSuccess ||
-        (nnz > 0 && cudaMemcpyAsync(d_items.p, h_items, (size_t)nnz * 4, cudaMemcpyHostToDevice, s) != cudaSuccess)) {
-        set_error("host-to-device copy of the transaction set failed");
-        return done(TFIM_E_CUDA);
-    }
+    if ((rc = d_stats.reserve(sizeof(ScanStats)))) return done(rc);
     hs.id_min = INT_MAX; hs.id_max = INT_MIN; hs.len_min = LLONG_MAX; hs.red_min = LLONG_MAX;
     cudaMemcpyAsync(d_stats.p, &hs, sizeof hs, cudaMemcpyHostToDevice, s);
-    if (nnz > 0) k_item_minmax<<<grid_for(nnz), 256, 0, s>>>(d_items.as<int32_t>(), nnz, d_stats.as<ScanStats>());
-    if (n_rows > 0) k_row_lengths<<<grid_for(n_rows), 256, 0, s>>>(d_off.as<int64_t>(), n_rows, d_stats.as<ScanStats>());
+    if (nnz > 0) k_item_minmax<<<grid_for(nnz), 256, 0, s>>>(d_items_p, nnz, d_stats.as<ScanStats>());
+    if (n_rows > 0) k_row_lengths<<<grid_for(n_rows), 256, 0, s>>>(d_off_p, n_rows, d_stats.as<ScanStats>());
     cudaMemcpyAsync(&hs, d_stats.p, sizeof hs, cudaMemcpyDeviceToHost, s);
     if (cudaStreamSynchronize(s) != cudaSuccess) { set_error("ingest statistics pass failed: %s", cudaGetErrorString(cudaGetLastError())); return done(TFIM_E_CUDA); }
     int64_t n_rows_all = n_rows;
@@ -320,11 +332,11 @@ int ingest_csr(tfim_ctx* c, const int64_t* h_off, const int32_t* h_items, int64_
                 cudaFuncSetAttribute(k_hist_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, kHistSmemBins * 4);
                 configured[dev].store(true);
             }
-            k_hist_smem<<<parts, 1024, (size_t)bins * 4, s>>>(d_items.as<int32_t>(), nnz, bins, d_tmp.as<int32_t>());
+            k_hist_smem<<<parts, 1024, (size_t)bins * 4, s>>>(d_items_p, nnz, bins, d_tmp.as<int32_t>());
             k_hist_sum<<<(bins + 255) / 256, 256, 0, s>>>(d_tmp.as<int32_t>(), parts, bins, d_freq.as<int32_t>());
         } else {
             cudaMemsetAsync(d_freq.p, 0, (size_t)bins * 4, s);
-            if (nnz > 0) k_hist<<<grid_for(nnz), 256, 0, s>>>(d_items.as<int32_t>(), nnz, d_freq.as<int32_t>());
+            if (nnz > 0) k_hist<<<grid_for(nnz), 256, 0, s>>>(d_items_p, nnz, d_freq.as<int32_t>());
         }
     }
     if ((rc = group_reduce(c, d_freq.p, id_max + 1, TFIM_DT_I32, TFIM_RED_SUM, s))) return done(rc);
@@ -390,7 +402,7 @@ int ingest_csr(tfim_ctx* c, const int64_t* h_off, const int32_t* h_items, int64_
     int64_t* item_off = red_idx + std::max<int64_t>(n_rows, 1);
     if (n_rows > 0) {
         int32_t* red_len = d_flag.as<int32_t>();
-        k_reduced_rows<<<grid_for(n_rows), 256, 0, s>>>(d_off.as<int64_t>(), d_items.as<int32_t>(), n_rows,
+        k_reduced_rows<<<grid_for(n_rows), 256, 0, s>>>(d_off_p, d_items_p, n_rows,
                                                          d_map.as<int32_t>(), red_len, d_stats.as<ScanStats>());
         cub::TransformInputIterator<int32_t, IsPositive, const int32_t*> flags(red_len, IsPositive());
         size_t tb1 = 0, tb2 = 0;
@@ -431,7 +443,7 @@ int ingest_csr(tfim_ctx* c, const int64_t* h_off, const int32_t* h_items, int64_
     c->n_red_items = n_red_items;
     cudaMemcpyAsync(c->d_red_off + n_red, &n_red_items, 8, cudaMemcpyHostToDevice, s);
     if (n_red > 0)
-        k_write_reduced<<<grid_for(n_rows), 256, 0, s>>>(d_off.as<int64_t>(), d_items.as<int32_t>(), n_rows, d_map.as<int32_t>(),
+        k_write_reduced<<<grid_for(n_rows), 256, 0, s>>>(d_off_p, d_items_p, n_rows, d_map.as<int32_t>(),
                                                           d_flag.as<int32_t>(), red_idx, item_off, c->d_red_off, c->d_red_items);
 
     // the bitmap: n_dense rows x W words, zero padded

@@ -151,7 +151,9 @@ struct Wave {
         j.n_rows = (int32_t)rs.size(); j.n_cols = (int32_t)cs.size();
         j.row_off = (int32_t)rows.size(); j.col_off = (int32_t)cols.size();
         j.out_off = out_total;
-        j.self_col = -1;
+        j.self_col = -1;   // a -1 column id is the all-ones column: tell the counters its index
+        for (int32_t q = 0; q < j.n_cols; q++)
+            if (cs[q] < 0) { j.self_col = q; break; }
         j.pad = 0;
         const int32_t id = (int32_t)jobs.size();
         jobs.push_back(j);

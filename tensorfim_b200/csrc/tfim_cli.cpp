@@ -21,78 +21,6 @@
 
 namespace {
 
-// The reference byte scanner (kernel_bitmap.cu:205-267): every '\n' ends a row (empty
-// rows included), runs of digits are ids, "-<digits>" is dropped, any other byte
-// separates, and a final row without '\n' counts only when it holds an id.  The file is
-// split at newlines into one chunk per thread; each chunk is scanned independently and the
-// per-chunk CSR pieces are concatenated.
-struct Chunk {
-    std::vector<int64_t> row_len;
-    std::vector<int32_t> items;
-};
-
-void scan(const char* p, const char* end, bool last, Chunk& out) {
-    int64_t len = 0;
-    while (p < end) {
-        const char ch = *p;
-        if (ch == '\n') { out.row_len.push_back(len); len = 0; p++; continue; }
-        if (ch >= '0' && ch <= '9') {
-            long v = 0;
-            while (p < end && *p >= '0' && *p <= '9') v = v * 10 + (*p++ - '0');
-            out.items.push_back((int32_t)v);
-            len++;
-            continue;
-        }
-        if (ch == '-') {
-            p++;
-            while (p < end && *p >= '0' && *p <= '9') p++;
-            continue;
-        }
-        p++;
-    }
-    if (last && len > 0) out.row_len.push_back(len);
-}
-
-bool parse_file(const char* path, std::vector<int64_t>& off, std::vector<int32_t>& items) {
-    FILE* fp = fopen(path, "rb");
-    if (!fp) return false;
-    fseeko(fp, 0, SEEK_END);
-    const long long sz = ftello(fp);
-    fseeko(fp, 0, SEEK_SET);
-    std::vector<char> buf(sz > 0 ? (size_t)sz : 1);
-    if (sz > 0 && fread(buf.data(), 1, (size_t)sz, fp) != (size_t)sz) { fclose(fp); return false; }
-    fclose(fp);
-    unsigned nt = std::thread::hardware_concurrency();
-    if (nt < 1) nt = 1;
-    if (sz < (1 << 22)) nt = 1;
-    // chunk boundaries just after a '\n'
-    std::vector<size_t> cut(1, 0);
-    for (unsigned t = 1; t < nt; t++) {
-        size_t pos = (size_t)sz * t / nt;
-        if (pos <= cut.back()) continue;
-        while (pos < (size_t)sz && buf[pos - 1] != '\n') pos++;
-        if (pos < (size_t)sz && pos > cut.back()) cut.push_back(pos);
-    }
-    cut.push_back((size_t)sz);
-    const size_t nc = cut.size() - 1;
-    std::vector<Chunk> parts(nc);
-    std::vector<std::thread> th;
-    for (size_t k = 0; k < nc; k++)
-        th.emplace_back([&, k] { scan(buf.data() + cut[k], buf.data() + cut[k + 1], k + 1 == nc, parts[k]); });
-    for (auto& t : th) t.join();
-    size_t rows = 0, n = 0;
-    for (auto& p : parts) { rows += p.row_len.size(); n += p.items.size(); }
-    off.assign(rows + 1, 0);
-    items.resize(n);
-    size_t r = 0, o = 0;
-    for (auto& p : parts) {
-        for (int64_t l : p.row_len) { off[r + 1] = off[r] + l; r++; }
-        memcpy(items.data() + o, p.items.data(), p.items.size() * 4);
-        o += p.items.size();
-    }
-    return true;
-}
-
 double now() { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); }
 
 // The proposal network's weights file (written by tensorfim_b200.learn): "TFIMMLP1", int32
@@ -163,18 +91,17 @@ int main(int argc, char** argv) {
         else if (k == "--superset") opts.superset = atoi(v.c_str());
         else { fprintf(stderr, "unknown option %s\n", k.c_str()); return 1; }
     }
-    const double t0 = now();
-    std::vector<int64_t> off;
-    std::vector<int32_t> items;
-    if (!parse_file(path, off, items)) {
+    // the file is read into pinned staging by worker threads, copied to the GPU in chunks and
+    // parsed there (the reference's readTransSetFile rules), then ingested on the GPU
+    const double t1 = now();
+    tfim_ctx* ctx = nullptr;
+    int rc = tfim_open_file(path, thr, 0, &ctx);
+    if (rc == TFIM_E_IO) {
         printf("%s open failed!\n", path);
         return 1;
     }
-    const double t1 = now();
-    tfim_ctx* ctx = nullptr;
-    int rc = tfim_open_db(off.data(), items.data(), (int64_t)off.size() - 1, thr, 0, &ctx);
     if (rc != TFIM_OK) {
-        fprintf(stderr, "tfim_open_db failed (%d): %s\n", rc, tfim_last_error());
+        fprintf(stderr, "tfim_open_file failed (%d): %s\n", rc, tfim_last_error());
         return 1;
     }
     const double t2 = now();
@@ -216,7 +143,6 @@ int main(int argc, char** argv) {
         return 1;
     }
     printf("======================================================================\n");
-    printf("parse_time(s): %g\n", t1 - t0);
     printf("preprocessing_time(s): %g\n", t2 - t1);
     printf("computation_time(s): %g\n", st.mine_seconds);
     printf("total_time(s): %g\n", t2 - t1 + st.mine_seconds);

@@ -318,6 +318,19 @@ void adopt_resident(tfim_ctx* c);
 int release_cached(int device);
 int mlp_device_params(tfim_mlp* h, const void** wbf, const float** params);
 int compute_bit_supports(tfim_ctx* ctx);
+// ingest from a CSR already in device memory (row_offsets[0] == 0, ids >= 0 checked)
+int ingest_device_csr(tfim_ctx* c, const int64_t* d_off, const int32_t* d_items, int64_t n_rows, int64_t nnz, double thr);
+// A transaction file's bytes as a source: either a host buffer or an open file descriptor
+// (read with pread), copied to the device in chunks through pinned staging.
+struct TextSource {
+    const char* host = nullptr;   // host bytes (pageable or pinned), or
+    int fd = -1;                  // a readable file descriptor
+    int64_t n_bytes = 0;
+};
+// Parse the file bytes on the device (reference readTransSetFile) into a device CSR:
+// *d_off (n_rows + 1 int64) and *d_items (max(nnz, 1) int32), both from dev_alloc on `s`.
+int parse_text_device(const TextSource& src, cudaStream_t s, int64_t** d_off, int32_t** d_items, int64_t* n_rows,
+                      int64_t* nnz);
 // Per-node prefix masks from item lists and one count job over every counted row (abi.cu):
 // counts[i][e] = popc(AND of node i's items & B[e]), nfreq[i] = #{e : counts >= min_count}.
 int count_wave_impl(tfim_ctx* c, int32_t b, int32_t min_count, const int32_t* d_items, const MatDesc* d_mats,

@@ -26,6 +26,26 @@ def _ptr(a: np.ndarray) -> C.c_void_p:
     return C.c_void_p(a.ctypes.data) if a.size else C.c_void_p(0)
 
 
+def _byte_view(data) -> np.ndarray:
+    if isinstance(data, np.ndarray):
+        return np.ascontiguousarray(data).view(np.uint8).reshape(-1)
+    return np.frombuffer(memoryview(data), dtype=np.uint8)
+
+
+def parse_text(data, device: int = 0) -> tuple[np.ndarray, np.ndarray]:
+    """The CSR (offsets int64, items int32) of a transaction file's bytes, parsed on the GPU
+    with the reference's scanner rules (tfim_parse_text)."""
+    buf = _byte_view(data)
+    rows, n = C.c_int64(), C.c_int64()
+    src = _ptr(buf) if buf.size else None
+    check(lib().tfim_parse_text(src, buf.size, device, None, 0, None, 0, C.byref(rows), C.byref(n)))
+    off = np.zeros(rows.value + 1, np.int64)
+    items = np.zeros(max(n.value, 1), np.int32)
+    check(lib().tfim_parse_text(src, buf.size, device, _ptr(off), off.size, _ptr(items), items.size, C.byref(rows),
+                                C.byref(n)))
+    return off, items[:n.value]
+
+
 def read_fimi(path: str) -> tuple[np.ndarray, np.ndarray]:
     """Parse a transaction file with the reference's byte-scanner rules
     (code/engine/src/kernel_bitmap.cu:205-233): every '\\n' ends a row (empty rows
@@ -148,8 +168,19 @@ class Database:
 
     @classmethod
     def from_file(cls, path: str, minsup: float, device: int = 0) -> "Database":
-        off, items = read_fimi(path)
-        return cls.from_csr(off, items, minsup, device)
+        """A transaction file, read into pinned staging and parsed on the GPU (tfim_open_file)."""
+        h = C.c_void_p()
+        check(lib().tfim_open_file(os.fsencode(path), float(minsup), device, C.byref(h)))
+        return cls(h, device)
+
+    @classmethod
+    def from_text(cls, data, minsup: float, device: int = 0) -> "Database":
+        """The bytes of a transaction file (bytes, bytearray or a uint8 array, pinned or not),
+        parsed on the GPU (tfim_open_text)."""
+        buf = _byte_view(data)
+        h = C.c_void_p()
+        check(lib().tfim_open_text(_ptr(buf) if buf.size else None, buf.size, float(minsup), device, C.byref(h)))
+        return cls(h, device)
 
     @classmethod
     def from_bitmap(cls, rows: np.ndarray, n_bits: int, n_counted: int, device: int = 0) -> "Database":

@@ -229,3 +229,28 @@ def test_family_counter_shared_memory_windows():
                 worst = max(worst, a_end, b_end)
     # the aligned base lies at most align - 1 bytes into the allocation
     assert worst + align - 1 <= smem
+
+
+def test_oracle_parse_matches_read_fimi_on_random_bytes(oracle_mod, tmp_path):
+    """The oracle's parse (the restated reference scanner, the checker of the GPU parse)
+    and the numpy reader agree on the golden input files and on random byte strings over
+    digits, '-', separators, CR and LF."""
+    names = sorted(f for f in os.listdir(os.path.join(ROOT, "tests", "golden")) if f.endswith(".txt"))
+    paths = [os.path.join(ROOT, "tests", "golden", f) for f in names]
+    rng = np.random.Generator(np.random.PCG64(11))
+    for k in range(20):
+        out = bytearray()
+        n = int(rng.integers(0, 3000))
+        while len(out) < n:
+            if rng.random() < 0.55:
+                out += bytes(rng.integers(48, 58, size=int(rng.integers(1, 19))).tolist())
+            else:
+                out += b" \t\r\n-,x\n"[int(rng.integers(0, 8)):][:1]
+        p = tmp_path / f"r{k}.txt"
+        p.write_bytes(bytes(out[:n]))
+        paths.append(str(p))
+    for path in paths:
+        a_off, a_items = oracle_mod.parse_file(path)
+        b_off, b_items = tf.read_fimi(path)
+        assert a_off.tolist() == b_off.tolist(), path
+        assert a_items.tolist() == b_items.tolist(), path
