@@ -192,16 +192,121 @@ __device__ void lop3_tile_impl(const CountArgs& a, const TileDesc t, Lop3Shared&
     __syncthreads();   // shared state is reused by the block's next tile
 }
 
-// Tiles of more than 32 columns give each lane two columns.
+// A tile of a dense family (flag bit 0 of TileDesc.pad, set by the resident pack when the
+// prefix holds at least 1/16 of the transactions): no 128-bit position is zero there, so the
+// skipping machinery above only costs L1 traffic (staged rows written and re-read, the base
+// and rows read twice).  Instead every thread owns a block of BR rows x BC columns and a
+// strided share of the slice's positions; per position it loads the base, its rows and its
+// columns straight from L2 (16-byte loads, consecutive positions on consecutive lanes) and
+// adds BR x BC popcounts held in registers -- (2 + BR + BC) loads per BR * BC popc4 instead of
+// about 1 + nr per nr.  The G threads of a block meet in shared memory at the end, as above.
+template <int BR>
+__device__ void lop3_dense_impl(const CountArgs& a, const TileDesc t, int32_t* sacc) {
+    constexpr int BC = BR == 1 ? 16 : BR == 2 ? 8 : BR == 3 ? 5 : 4;
+    const JobDesc j = a.jobs[t.job];
+    const int64_t W = a.W;
+    const int tid = threadIdx.x;
+    const int nr = t.nr, nc = t.c1 - t.c0;
+    const int rb = (nr + BR - 1) / BR, cb = (nc + BC - 1) / BC, nb = rb * cb;   // at most 2 x 16
+    const int G = blockDim.x / nb;
+    const int b = tid / G, g = tid - b * G;
+    const bool busy = b < nb;
+    const int br = busy ? (b / cb) * BR : 0, bc = busy ? (b % cb) * BC : 0;
+    for (int q = tid; q < kLop3Rows * 64; q += blockDim.x) sacc[q] = 0;
+    const uint4* base_m = j.base_slot >= 0 ? reinterpret_cast<const uint4*>(a.masks + (int64_t)j.base_slot * W) : nullptr;
+    const uint4* base_i = j.base_item >= 0 ? reinterpret_cast<const uint4*>(a.bitmap + (int64_t)j.base_item * W) : nullptr;
+    // sources of the block's rows and columns, clamped to the tile's last row / column (pairs
+    // outside the tile are computed on valid rows and discarded); a null source is all ones
+    const uint4* rsl[BR];
+    const uint4* rit[BR];
+    const uint4* csrc[BC];
+#pragma unroll
+    for (int x = 0; x < BR; x++) {
+        const RowDesc rd = a.rows[j.row_off + t.r0 + min(br + x, nr - 1)];
+        rsl[x] = rd.slot >= 0 ? reinterpret_cast<const uint4*>(a.masks + (int64_t)rd.slot * W) : nullptr;
+        rit[x] = rd.item >= 0 ? reinterpret_cast<const uint4*>(a.bitmap + (int64_t)rd.item * W) : nullptr;
+    }
+#pragma unroll
+    for (int y = 0; y < BC; y++) {
+        const int c = t.c0 + min(bc + y, nc - 1);
+        const int32_t col = c == j.self_col ? -1 : a.cols[j.col_off + c];
+        csrc[y] = col >= 0 ? reinterpret_cast<const uint4*>(a.bitmap + (int64_t)col * W) : nullptr;
+    }
+    uint32_t acc[BR][BC];
+#pragma unroll
+    for (int x = 0; x < BR; x++)
+#pragma unroll
+        for (int y = 0; y < BC; y++) acc[x][y] = 0;
+    __syncthreads();   // sacc cleared
+    const uint4 ones = make_uint4(~0u, ~0u, ~0u, ~0u);
+    const int64_t P0 = t.w0 >> 2, P1 = t.w1 >> 2;
+    if (busy) {
+        for (int64_t p = P0 + g; p < P1; p += G) {
+            uint4 base = ones;
+            if (base_m) base = and4(base, __ldg(base_m + p));
+            if (base_i) base = and4(base, __ldg(base_i + p));
+            uint4 xr[BR];
+#pragma unroll
+            for (int x = 0; x < BR; x++) {
+                uint4 v = base;
+                if (rsl[x]) v = and4(v, __ldg(rsl[x] + p));
+                if (rit[x]) v = and4(v, __ldg(rit[x] + p));
+                xr[x] = v;
+            }
+#pragma unroll
+            for (int y = 0; y < BC; y++) {
+                const uint4 cv = csrc[y] ? __ldg(csrc[y] + p) : ones;
+#pragma unroll
+                for (int x = 0; x < BR; x++) acc[x][y] += popc4(and4(xr[x], cv));
+            }
+        }
+#pragma unroll
+        for (int x = 0; x < BR; x++)
+#pragma unroll
+            for (int y = 0; y < BC; y++)
+                if (br + x < nr && bc + y < nc && acc[x][y]) atomicAdd(&sacc[(br + x) * 64 + bc + y], (int32_t)acc[x][y]);
+    }
+    __syncthreads();
+    for (int q = tid; q < nr * nc; q += blockDim.x) {
+        const int r = q / nc, c = q - r * nc;
+        const int32_t v = sacc[r * 64 + c];
+        if (v) atomicAdd(a.out + j.out_off + (int64_t)(t.r0 + r) * j.n_cols + t.c0 + c, v);
+    }
+    __syncthreads();   // shared state is reused by the block's next tile
+}
+
+// Row blocks by the tile's rows: 1, 2, 3 (also 5, 6 as two blocks) or 4 (also 7, 8).
+__device__ __forceinline__ void lop3_dense_tile(const CountArgs& a, const TileDesc t, int32_t* sacc) {
+    switch (t.nr) {
+        case 1: lop3_dense_impl<1>(a, t, sacc); break;
+        case 2: lop3_dense_impl<2>(a, t, sacc); break;
+        case 3: case 5: case 6: lop3_dense_impl<3>(a, t, sacc); break;
+        default: lop3_dense_impl<4>(a, t, sacc); break;
+    }
+}
+
+// Tiles of more than 32 columns give each lane two columns.  DENSE: the launch may hold
+// dense tiles too (the persistent form); the plain launches hold one kind each.
+template <bool DENSE>
 __device__ __forceinline__ void lop3_tile(const CountArgs& a, const TileDesc t, Lop3Shared& sh) {
-    if (t.c1 - t.c0 > 32) lop3_tile_impl<true>(a, t, sh);
+    if (DENSE && (t.pad & 1)) lop3_dense_tile(a, t, sh.acc);
+    else if (t.c1 - t.c0 > 32) lop3_tile_impl<true>(a, t, sh);
     else lop3_tile_impl<false>(a, t, sh);
 }
 
 __global__ void __launch_bounds__(256, 4) k_count_lop3(CountArgs a) {
     __shared__ Lop3Shared sh;
     phase_begin(a.ph_s);
-    lop3_tile(a, a.tiles[blockIdx.x], sh);
+    lop3_tile<false>(a, a.tiles[blockIdx.x], sh);
+    phase_end(a.ph_e);
+}
+
+// Dense tiles only (a separate launch, so that the register budget of the skipping tiles
+// above stays as it is).
+__global__ void __launch_bounds__(256, 3) k_count_lop3_dense(CountArgs a) {
+    __shared__ int32_t sacc[kLop3Rows * 64];
+    phase_begin(a.ph_s);
+    lop3_dense_tile(a, a.tiles[blockIdx.x], sacc);
     phase_end(a.ph_e);
 }
 
@@ -221,7 +326,7 @@ __global__ void __launch_bounds__(256, 4) k_count_lop3_persistent(const CountArg
         const int32_t t = s_t;
         __syncthreads();
         if (t >= n) break;
-        lop3_tile(a, a.tiles[t], sh);
+        lop3_tile<true>(a, a.tiles[t], sh);
     }
     phase_end(a.ph_e);
 }
@@ -296,6 +401,13 @@ __global__ void k_compact(const int32_t* __restrict__ counts, const JobDesc* __r
 int launch_count_lop3(const CountArgs& a, cudaStream_t s) {
     if (a.n_tiles <= 0) return TFIM_OK;
     k_count_lop3<<<a.n_tiles, 256, 0, s>>>(a);
+    TFIM_CUDA(cudaGetLastError());
+    return TFIM_OK;
+}
+
+int launch_count_lop3_dense(const CountArgs& a, cudaStream_t s) {
+    if (a.n_tiles <= 0) return TFIM_OK;
+    k_count_lop3_dense<<<a.n_tiles, 256, 0, s>>>(a);
     TFIM_CUDA(cudaGetLastError());
     return TFIM_OK;
 }

@@ -58,6 +58,8 @@ struct DJob {
                                // jobs' (prefix b3l after all heavy tiles)
     int32_t btc;               // exclusive prefix of the tcgen05 family counter's jobs
     int32_t bgr;               // exclusive prefix of the CUDA-core Gram counter's jobs
+    int32_t b3d;               // CUDA-core tiles of dense families (heavy == 2): they come before all
+                               // others (prefix b3d), for the register-blocked dense launch
 };
 
 // Phases of a wave (device-time stamps) and counter classes of a count job.
@@ -73,7 +75,8 @@ struct ResStatus {
     // g_* fields hold its size, for the host to grow the pools and pack again
     int32_t grow, g_rows, g_jobs, g_max_head, g_max_cols, waves;
     int64_t g_out, g_tiles;
-    int32_t launch_id, next3, next1, pad1;   // next3 / next1: tile counters of the persistent counters
+    int32_t launch_id, next3, next1;         // next3 / next1: tile counters of the persistent counters
+    int32_t tiles_l3d;                       // the first tiles_l3d CUDA-core tiles are dense families'
     int32_t tiles_tc, next_tc;               // tcgen05 family counter: tiles, tile counter
     int32_t tiles_gr, next_gr;               // CUDA-core Gram counter: tiles, tile counter
     unsigned long long launch_t0;
@@ -268,7 +271,12 @@ __device__ __forceinline__ int find_job_by_tile(const DJob* dj, int nj, int64_t 
     int lo = 0, hi = nj - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
-        const int32_t v = K == 0 ? dj[mid].b3 : K == 1 ? dj[mid].b1 : K == 2 ? dj[mid].b3l : K == 3 ? dj[mid].btc : dj[mid].bgr;
+        const int32_t v = K == 0   ? dj[mid].b3
+                          : K == 1 ? dj[mid].b1
+                          : K == 2 ? dj[mid].b3l
+                          : K == 3 ? dj[mid].btc
+                          : K == 4 ? dj[mid].bgr
+                                   : dj[mid].b3d;
         if (v <= t) lo = mid; else hi = mid - 1;
     }
     return lo;
@@ -343,7 +351,7 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
             const DFam f = p.fams[L.fam];
             DJob dj;
             dj.fam = L.fam; dj.kind = kJobLook; dj.r0 = 0; dj.nr = 1; dj.slot = L.slot; dj.log = L.log; dj.b3 = 0; dj.b1 = 0;
-            dj.cls = 0; dj.sl3 = 1; dj.b3l = 0; dj.heavy = 0; dj.btc = 0; dj.bgr = 0;
+            dj.cls = 0; dj.sl3 = 1; dj.b3l = 0; dj.heavy = 0; dj.btc = 0; dj.bgr = 0; dj.b3d = 0;
             p.djobs[k] = dj;
             JobDesc jd;
             jd.base_slot = -1; jd.base_item = -1; jd.n_rows = 1; jd.n_cols = f.nF - f.nT + 1;
@@ -447,7 +455,7 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
             const int32_t jid = s_n_jobs + (int32_t)hx[q];
             DJob dj;
             dj.fam = fid; dj.kind = kJobFam; dj.r0 = f.next_row; dj.nr = take[q]; dj.slot = -1; dj.log = -1; dj.b3 = 0; dj.b1 = 0;
-            dj.cls = 0; dj.sl3 = 1; dj.b3l = 0; dj.heavy = 0; dj.btc = 0; dj.bgr = 0;
+            dj.cls = 0; dj.sl3 = 1; dj.b3l = 0; dj.heavy = 0; dj.btc = 0; dj.bgr = 0; dj.b3d = 0;
             p.djobs[jid] = dj;
             JobDesc jd;
             jd.base_slot = f.slot; jd.base_item = f.item; jd.n_rows = take[q]; jd.n_cols = f.nF;
@@ -569,14 +577,16 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
     // about 8 tile slices per SM: two rounds of the 4 resident blocks
     const float target = fmaxf(s_cost / (p.l3_slices_per_sm * (float)p.sm_count), 1.f);
     const int64_t max_sl = lmax(1, W / 256);
-    // heavy jobs (cost at least half the slice target) first, so that the longest tiles are
-    // dispatched first and the light ones fill in behind them
-    int64_t tot3h = 0, tot3l = 0;
+    // Tiles of dense families (the prefix holds at least 1/16 of the transactions, so no
+    // 128-bit position is zero to skip) come first, for the register-blocked dense launch;
+    // then heavy jobs (cost at least half the slice target), so that the longest tiles are
+    // dispatched first and the light ones fill in behind them.
+    int64_t tot3d = 0, tot3h = 0, tot3l = 0;
     for (int base = 0; base < nj; base += kPackCand) {
-        int64_t ah[kPackItems], al[kPackItems], xh[kPackItems], xl[kPackItems];
+        int64_t ad[kPackItems], ah[kPackItems], al[kPackItems], xd[kPackItems], xh[kPackItems], xl[kPackItems];
         for (int q = 0; q < kPackItems; q++) {
             const int j = base + tid * kPackItems + q;
-            ah[q] = al[q] = 0;
+            ad[q] = ah[q] = al[q] = 0;
             if (j < nj) {
                 const JobDesc jd = p.jobs[j];
                 DJob* djp = p.djobs + j;
@@ -586,12 +596,18 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
                     const int64_t wsl = ((W / 64 + sl - 1) / sl) * 64;
                     sl = wsl > 0 ? (W + wsl - 1) / wsl : 1;
                     djp->sl3 = (int32_t)sl;
-                    djp->heavy = cost >= 0.5f * target ? 1 : 0;
-                    if (djp->heavy) ah[q] = l3_tiles(jd.n_rows, jd.n_cols) * sl;
-                    else al[q] = l3_tiles(jd.n_rows, jd.n_cols) * sl;
+                    const bool dense = djp->kind == kJobFam && 16 * (int64_t)p.fams[djp->fam].sup >= p.n_bits;
+                    djp->heavy = dense ? 2 : cost >= 0.5f * target ? 1 : 0;
+                    const int64_t nt = l3_tiles(jd.n_rows, jd.n_cols) * sl;
+                    if (djp->heavy == 2) ad[q] = nt;
+                    else if (djp->heavy) ah[q] = nt;
+                    else al[q] = nt;
                 }
             }
         }
+        Scan(tmp.scan).ExclusiveSum(ad, xd, s_agg);
+        __syncthreads();
+        const int64_t gd = s_agg;
         Scan(tmp.scan).ExclusiveSum(ah, xh, s_agg);
         __syncthreads();
         const int64_t gh = s_agg;
@@ -601,15 +617,17 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
         for (int q = 0; q < kPackItems; q++) {
             const int j = base + tid * kPackItems + q;
             if (j < nj) {
+                p.djobs[j].b3d = (int32_t)(tot3d + xd[q]);
                 p.djobs[j].b3 = (int32_t)(tot3h + xh[q]);
                 p.djobs[j].b3l = (int32_t)(tot3l + xl[q]);
             }
         }
+        tot3d += gd;
         tot3h += gh;
         tot3l += gl;
         __syncthreads();
     }
-    const int64_t tot3 = tot3h + tot3l;
+    const int64_t tot3 = tot3d + tot3h + tot3l;
     const int64_t want1 = lmax(1, (int64_t)(p.b1_tiles_per_sm * (float)p.sm_count));
     int64_t ks1 = tot1 > 0 ? lmax(1, (want1 + tot1 - 1) / tot1) : 1;
     ks1 = lmin(ks1, lmax(1, W / 64));
@@ -652,7 +670,8 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
     __syncthreads();
     if (!s_fit) {
         if (tid == 0) {
-            st->jobs = 0; st->rows = 0; st->tiles_l3 = 0; st->tiles_b1 = 0; st->tiles_tc = 0; st->tiles_gr = 0; st->n_proj = 0;
+            st->jobs = 0; st->rows = 0; st->tiles_l3 = 0; st->tiles_l3d = 0; st->tiles_b1 = 0; st->tiles_tc = 0;
+            st->tiles_gr = 0; st->n_proj = 0;
             st->out_total = 0;
             st->ph_e[kPhPack] = globaltimer();
         }
@@ -703,11 +722,13 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
     }
     if (T3 <= p.cap_tiles)
         for (int64_t t = tid; t < T3; t += kPackThreads) {
-            const bool hv = t < tot3h;
-            const int j = hv ? find_job_by_tile<0>(p.djobs, nj, t) : find_job_by_tile<2>(p.djobs, nj, t - tot3h);
+            const int grp = t < tot3d ? 0 : t < tot3d + tot3h ? 1 : 2;   // dense, heavy, light
+            const int j = grp == 0   ? find_job_by_tile<5>(p.djobs, nj, t)
+                          : grp == 1 ? find_job_by_tile<0>(p.djobs, nj, t - tot3d)
+                                     : find_job_by_tile<2>(p.djobs, nj, t - tot3d - tot3h);
             const JobDesc jd = p.jobs[j];
             const DJob dj = p.djobs[j];
-            const int64_t local = hv ? t - dj.b3 : t - tot3h - dj.b3l;
+            const int64_t local = grp == 0 ? t - dj.b3d : grp == 1 ? t - tot3d - dj.b3 : t - tot3d - tot3h - dj.b3l;
             const int64_t bt = l3_tiles(jd.n_rows, jd.n_cols);
             const int64_t slice = local / bt, within = local % bt;
             const int64_t wsl = ((W / 64 + dj.sl3 - 1) / dj.sl3) * 64;
@@ -715,7 +736,7 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
             const int rg = (int)(within / cg), cc = (int)(within % cg);
             const int64_t w0 = slice * wsl;
             p.tiles_l3[t] = TileDesc{j, rg * kLop3Rows, min(kLop3Rows, jd.n_rows - rg * kLop3Rows), cc * 64,
-                                     min(jd.n_cols, cc * 64 + 64), (int32_t)w0, (int32_t)lmin(W, w0 + wsl), 0};
+                                     min(jd.n_cols, cc * 64 + 64), (int32_t)w0, (int32_t)lmin(W, w0 + wsl), grp == 0 ? 1 : 0};
         }
     if (T1 <= p.cap_tiles)
         for (int64_t t = tid; t < T1; t += kPackThreads) {
@@ -752,6 +773,7 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
         st->jobs = nj;
         st->rows = rows_total;
         st->tiles_l3 = (int32_t)T3;
+        st->tiles_l3d = (int32_t)tot3d;
         st->tiles_b1 = (int32_t)T1;
         st->tiles_tc = (int32_t)TT;
         st->tiles_gr = (int32_t)TG;
@@ -2272,12 +2294,22 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
         a.bitmap = c->d_bitmap; a.W = W; a.masks = c->d_masks.as<uint32_t>(); a.jobs = P.jobs; a.rows = P.rows;
         a.cols = P.items; a.out = P.counts; a.job_list = P.proj_list;
         if (hst->tiles_l3) {
-            a.tiles = P.tiles_l3;
-            a.n_tiles = hst->tiles_l3;
+            // dense families' tiles (the first tiles_l3d), then the zero-skipping ones
             a.ph_s = &d_st->ph_s[kPhLop3]; a.ph_e = &d_st->ph_e[kPhLop3];
-            TFIM_TRY(launch_count_lop3(a, s));
-            launches++;
-            count_launches++;
+            if (hst->tiles_l3d) {
+                a.tiles = P.tiles_l3;
+                a.n_tiles = hst->tiles_l3d;
+                TFIM_TRY(launch_count_lop3_dense(a, s));
+                launches++;
+                count_launches++;
+            }
+            if (hst->tiles_l3 > hst->tiles_l3d) {
+                a.tiles = P.tiles_l3 + hst->tiles_l3d;
+                a.n_tiles = hst->tiles_l3 - hst->tiles_l3d;
+                TFIM_TRY(launch_count_lop3(a, s));
+                launches++;
+                count_launches++;
+            }
             path_launches[TFIM_PATH_LOP3]++;
         }
         if (hst->tiles_b1) {

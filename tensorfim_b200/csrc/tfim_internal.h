@@ -159,6 +159,8 @@ __device__ __forceinline__ void phase_end(unsigned long long* e) {
 }
 
 int launch_count_lop3(const CountArgs& a, cudaStream_t s);
+// tiles flagged dense (TileDesc.pad bit 0): register-blocked, no zero-position skipping
+int launch_count_lop3_dense(const CountArgs& a, cudaStream_t s);
 int launch_count_b1(const CountArgs& a, cudaStream_t s);
 // Persistent forms for waves built on the GPU: the arguments and the tile / job count are
 // read from device memory and a fixed grid strides over the tiles, so the launches do not
