@@ -306,6 +306,7 @@ def main() -> int:
     e2e = None
     if not args.no_e2e:
         e2e_ms, ph = [], {"open_ms": [], "mine_ms": [], "close_ms": []}
+        first_paths = []
         d2h = 0
         n_e2e = max(3, args.steps)
         for k in range(max(1, args.warmup) + n_e2e):
@@ -326,12 +327,17 @@ def main() -> int:
                 ph.setdefault("mine_device_ms", []).append(res.stats["device_ms"])
                 ph.setdefault("mine_readback_ms", []).append(res.stats["readback_ms"])
                 ph.setdefault("mine_setup_ms", []).append(res.stats["setup_ms"])
+                # where the first mine on a freshly opened database spends its time
+                for key in ("kernel_ms", "host_ms", "sync_ms", "top_ms", "pack_ms", "expand_ms", "mask_ms"):
+                    ph.setdefault("mine_" + key, []).append(res.stats[key])
+                first_paths.append(res.stats["path_ms"])
             d2h = res.items.nbytes + res.offsets.nbytes + res.supports.nbytes
         e2e_t = max_over_ranks(statistics.mean(e2e_ms))
         e2e = {"value": replicas.job_throughput(ref_supports, e2e_t, world), "unit": "supports/s",
                "h2d_bytes_per_step": int(h2d_bytes), "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_t,
                "steps": len(e2e_ms),
                "phases_ms": {k: statistics.mean(v) for k, v in ph.items()},
+               "mine_path_ms": [statistics.mean(x[q] for x in first_paths) for q in range(len(first_paths[0]))],
                "timing": "host wall clock around open (H2D of the pinned CSR + device ingest) + mine (search, MFI "
                          "read-back into host memory) + close"}
         if plain_ms is not None:

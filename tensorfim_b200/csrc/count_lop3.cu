@@ -303,7 +303,7 @@ __global__ void __launch_bounds__(256, 4) k_count_lop3(CountArgs a) {
 
 // Dense tiles only (a separate launch, so that the register budget of the skipping tiles
 // above stays as it is).
-__global__ void __launch_bounds__(256, 3) k_count_lop3_dense(CountArgs a) {
+__global__ void __launch_bounds__(256, 4) k_count_lop3_dense(CountArgs a) {
     __shared__ int32_t sacc[kLop3Rows * 64];
     phase_begin(a.ph_s);
     lop3_dense_tile(a, a.tiles[blockIdx.x], sacc);
