@@ -302,6 +302,11 @@ def main() -> int:
                               "lookahead_hits": last.stats["lookahead_hits"], "waves": last.stats["waves"],
                               "identical": last.as_dict() == batched.as_dict()}
 
+    # the benchmark database is closed before the end-to-end steps, as a caller opening
+    # databases in sequence would: with both open, two sets of search pools (tens of GB on
+    # this workload) exceed the device pool's cache and every step remaps memory
+    db.close()
+
     # end to end through the C ABI from pinned host memory
     e2e = None
     if not args.no_e2e:
@@ -408,7 +413,6 @@ def main() -> int:
         "gpu_launches": gpu_launches,
         "clocks": clk,
     }
-    db.close()
     if rank == 0:
         print(json.dumps(out))
     if world > 1:

@@ -155,6 +155,23 @@ def test_cfg3_replicated_matches_base_scaled():
     assert len(a) > 10
 
 
+@pytest.mark.slow
+def test_dense_full_size_matches_reference_fixture(tmp_path):
+    """The benchmark's dense database at full size -- 49,000 base rows x 256 exact replicas =
+    12,544,000 transactions, minsup 6% -- mined from its text file (device parse) by the
+    resident engine with the learned proposal, host and graph wave loops: the reference's
+    MFIs of the base rows (tests/golden/cfg3_base_t06, produced by the reference engine)
+    with every support x 256."""
+    fx = load_golden("cfg3_base_t06")
+    want = {k: v * 256 for k, v in fx["expected"].items()}
+    p = str(tmp_path / "dense.txt")
+    synth.write_fimi_replicated(p, synth.cfg3_base(), 256)
+    with tf.Database.from_file(p, synth.CFG3_DEVIATION_MINSUP) as db:
+        assert db.info["trans_num"] == 12_544_000
+        for graphs in (False, True):
+            assert db.mine(engine="resident", lookahead="learned", graphs=graphs).as_dict() == want, graphs
+
+
 @pytest.mark.parametrize("name", ["cfg1_full", "cfg4_s001", "cfg5_s002", "edge_ties", "cfg3_base"])
 def test_any_tuning_keeps_output(tmp_path, name):
     """The tuning table changes launch shapes and counter choices, never the MFI set."""
