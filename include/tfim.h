@@ -345,6 +345,8 @@ typedef struct {
     float   tc_tiles_per_sm;    /* tcgen05 family counter: word-slice tiles per SM and wave */
     int32_t gram_min_rows;      /* automatic choice: the CUDA-core Gram counter for dense family
                                    jobs of at most 64 columns and at least this many rows */
+    float   l3_dense_slices_per_sm; /* CUDA-core work split of dense families' tiles (resident
+                                   engine): tile slices per SM and wave */
 } tfim_tuning;
 
 /* The table in force (built-in values, or the loaded / set table). */

@@ -85,7 +85,7 @@ class Tuning(C.Structure):
                 ("rate_b1_bitops", C.c_double), ("rate_lop3_bitops", C.c_double), ("rate_pair_incr", C.c_double),
                 ("i8_min_rows", C.c_int32), ("i8_min_cols", C.c_int32), ("rate_i8_bitops", C.c_double),
                 ("tc_min_work", C.c_int32), ("tc_min_density", C.c_float), ("tc_tiles_per_sm", C.c_float),
-                ("gram_min_rows", C.c_int32)]
+                ("gram_min_rows", C.c_int32), ("l3_dense_slices_per_sm", C.c_float)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}

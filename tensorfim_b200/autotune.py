@@ -4,11 +4,11 @@ GPU and writes the tuning table the library loads (tensorfim_b200/tuning.json).
     python -m tensorfim_b200.autotune [--out PATH] [--reps 5] [--quick]
 
 Parameters (the tfim_tuning table of include/tfim.h):
-  * wave_rows, l3_slices_per_sm, b1_tiles_per_sm, b1_min (b1_min_rows = b1_min_cols):
-    coordinate descent over a grid, objective = the sum over the benchmark databases
-    (configurations 1, 4 and 5 of tensorfim_b200.synth with their minimum supports, plus
-    configuration 4 at 25% of its rows) of the median resident mine time with the learned
-    proposal;
+  * wave_rows, l3_slices_per_sm, l3_dense_slices_per_sm, b1_tiles_per_sm, b1_min
+    (b1_min_rows = b1_min_cols): coordinate descent over a grid, objective = the sum over the
+    benchmark databases (configurations 1, 4 and 5 of tensorfim_b200.synth with their minimum
+    supports, configuration 4 at 25% of its rows, and the dense replicated configuration at
+    64 replicas with minsup 6%) of the median resident mine time with the learned proposal;
   * rate_b1_bitops, rate_lop3_bitops, rate_i8_bitops: bit-ops/s of one 256-node x 512-item
     counting wave over a random half-dense bitmap of 2^18 transactions, each counter forced
     (tensorfim_b200.countbench);
@@ -36,10 +36,11 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 TABLE = os.path.join(HERE, "tuning.json")
 
 DATABASES = [("cfg4", 4, {}, 0.0005), ("cfg4_s025", 4, {"scale": 0.25}, 0.0005), ("cfg1", 1, {}, 0.10),
-             ("cfg5", 5, {}, 0.70)]
+             ("cfg5", 5, {}, 0.70), ("dense_r64", 3, {"replicas": 64}, 0.06)]
 GRID = {
     "wave_rows": [1024, 2048, 4096, 8192, 16384],
     "l3_slices_per_sm": [4.0, 8.0, 16.0, 32.0],
+    "l3_dense_slices_per_sm": [32.0, 64.0, 128.0, 192.0],
     "b1_tiles_per_sm": [2.0, 4.0, 8.0, 16.0],
     "b1_min": [8, 16, 32, 64],
 }
@@ -121,6 +122,7 @@ def main() -> None:
         db.mine(engine="resident", lookahead="learned")
 
     best = {"wave_rows": start["wave_rows"], "l3_slices_per_sm": start["l3_slices_per_sm"],
+            "l3_dense_slices_per_sm": start["l3_dense_slices_per_sm"],
             "b1_tiles_per_sm": start["b1_tiles_per_sm"], "b1_min": start["b1_min_rows"]}
     _apply(best)
     best_obj, _ = _objective(dbs, reps, ref)
@@ -147,7 +149,10 @@ def main() -> None:
              "b1_min_cols": int(best["b1_min"]), "proj_auto": int(start["proj_auto"]),
              "rate_b1_bitops": float(rates["rate_b1_bitops"]), "rate_lop3_bitops": float(rates["rate_lop3_bitops"]),
              "rate_pair_incr": float(rates["rate_pair_incr"]), "i8_min_rows": int(i8_min), "i8_min_cols": int(i8_min),
-             "rate_i8_bitops": float(rates["rate_i8_bitops"])}
+             "rate_i8_bitops": float(rates["rate_i8_bitops"]),
+             "l3_dense_slices_per_sm": float(best["l3_dense_slices_per_sm"])}
+    for k in ("tc_min_work", "tc_min_density", "tc_tiles_per_sm", "gram_min_rows"):   # not swept here
+        table[k] = start[k]
     import torch
     doc = dict(table)
     doc["measured_on"] = torch.cuda.get_device_name(0)

@@ -163,6 +163,7 @@ void tuning_builtin(tfim_tuning* t) {
     t->tc_min_density = 0.5f;
     t->tc_tiles_per_sm = 8.f;
     t->gram_min_rows = 16;
+    t->l3_dense_slices_per_sm = 128.f;
 }
 
 bool tuning_valid(const tfim_tuning& t) {
@@ -171,7 +172,7 @@ bool tuning_valid(const tfim_tuning& t) {
            (t.proj_auto == 0 || t.proj_auto == 1) && t.rate_b1_bitops > 0 && t.rate_lop3_bitops > 0 && t.rate_pair_incr > 0 &&
            t.i8_min_rows >= 1 && t.i8_min_cols >= 1 && t.rate_i8_bitops > 0 && t.tc_min_work >= 1 &&
            t.tc_min_density >= 0.f && t.tc_min_density <= 2.f && t.tc_tiles_per_sm > 0.f && t.tc_tiles_per_sm <= 1024.f &&
-           t.gram_min_rows >= 1;
+           t.gram_min_rows >= 1 && t.l3_dense_slices_per_sm > 0.f && t.l3_dense_slices_per_sm <= 1024.f;
 }
 
 // Flat JSON object of numbers: {"key": value, ...}.  Unknown keys are ignored.
@@ -184,7 +185,8 @@ int tuning_parse(const std::string& text, tfim_tuning* t) {
                         {"rate_pair_incr", 2, &t->rate_pair_incr}, {"i8_min_rows", 0, &t->i8_min_rows},
                         {"i8_min_cols", 0, &t->i8_min_cols}, {"rate_i8_bitops", 2, &t->rate_i8_bitops},
                         {"tc_min_work", 0, &t->tc_min_work}, {"tc_min_density", 1, &t->tc_min_density},
-                        {"tc_tiles_per_sm", 1, &t->tc_tiles_per_sm}, {"gram_min_rows", 0, &t->gram_min_rows}};
+                        {"tc_tiles_per_sm", 1, &t->tc_tiles_per_sm}, {"gram_min_rows", 0, &t->gram_min_rows},
+                        {"l3_dense_slices_per_sm", 1, &t->l3_dense_slices_per_sm}};
     for (const Key& k : keys) {
         const std::string pat = std::string("\"") + k.name + "\"";
         const size_t at = text.find(pat);

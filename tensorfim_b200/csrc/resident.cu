@@ -156,6 +156,7 @@ struct ResPtrs {
     int32_t proj_auto;            // let the automatic counter choice pick the projected counter
     int32_t b1_min_rows, b1_min_cols;   // automatic choice: tensor path from this job shape
     float l3_slices_per_sm, b1_tiles_per_sm;   // work split targets per wave
+    float l3_dense_slices_per_sm;               // ... of dense families' CUDA-core tiles
     int32_t tc_min_work;                       // automatic choice of the tcgen05 family counter
     float tc_min_density, tc_tiles_per_sm;
     int32_t gram_min_rows;                     // ... and of the CUDA-core Gram counter
@@ -574,8 +575,11 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
         if (tid == 0) s_cost = c;
         __syncthreads();
     }
-    // about 8 tile slices per SM: two rounds of the 4 resident blocks
+    // the wave's estimated CUDA-core cost over (slices per SM x SMs): the cost of one tile
+    // slice; dense families are split more finely (their own target), which shortens the
+    // launch's tail on large dense databases
     const float target = fmaxf(s_cost / (p.l3_slices_per_sm * (float)p.sm_count), 1.f);
+    const float target_d = fmaxf(s_cost / (p.l3_dense_slices_per_sm * (float)p.sm_count), 1.f);
     const int64_t max_sl = lmax(1, W / 256);
     // Tiles of dense families (the prefix holds at least 1/16 of the transactions, so no
     // 128-bit position is zero to skip) come first, for the register-blocked dense launch;
@@ -592,11 +596,11 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
                 DJob* djp = p.djobs + j;
                 if (djp->cls == 0) {
                     const float cost = l3_cost(jd, *djp);
-                    int64_t sl = lmin(max_sl, lmax(1, (int64_t)ceilf(cost / target)));
+                    const bool dense = djp->kind == kJobFam && 16 * (int64_t)p.fams[djp->fam].sup >= p.n_bits;
+                    int64_t sl = lmin(max_sl, lmax(1, (int64_t)ceilf(cost / (dense ? target_d : target))));
                     const int64_t wsl = ((W / 64 + sl - 1) / sl) * 64;
                     sl = wsl > 0 ? (W + wsl - 1) / wsl : 1;
                     djp->sl3 = (int32_t)sl;
-                    const bool dense = djp->kind == kJobFam && 16 * (int64_t)p.fams[djp->fam].sup >= p.n_bits;
                     djp->heavy = dense ? 2 : cost >= 0.5f * target ? 1 : 0;
                     const int64_t nt = l3_tiles(jd.n_rows, jd.n_cols) * sl;
                     if (djp->heavy == 2) ad[q] = nt;
@@ -2035,6 +2039,7 @@ int mine_resident(tfim_ctx* c, const tfim_mine_opts* o, tfim_mine_stats* stt) {
         P.b1_min_rows = tn.b1_min_rows;
         P.b1_min_cols = tn.b1_min_cols;
         P.l3_slices_per_sm = tn.l3_slices_per_sm;
+        P.l3_dense_slices_per_sm = tn.l3_dense_slices_per_sm;
         P.b1_tiles_per_sm = tn.b1_tiles_per_sm;
         P.tc_min_work = tn.tc_min_work;
         P.tc_min_density = tn.tc_min_density;
