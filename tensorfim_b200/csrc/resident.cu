@@ -581,8 +581,9 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
     const float target = fmaxf(s_cost / (p.l3_slices_per_sm * (float)p.sm_count), 1.f);
     const float target_d = fmaxf(s_cost / (p.l3_dense_slices_per_sm * (float)p.sm_count), 1.f);
     const int64_t max_sl = lmax(1, W / 256);
-    // Tiles of dense families (the prefix holds at least 1/16 of the transactions, so no
-    // 128-bit position is zero to skip) come first, for the register-blocked dense launch;
+    // Tiles of dense families and of their lookaheads (the family's prefix holds at least 1/16
+    // of the transactions, so no 128-bit position is zero to skip) come first, for the
+    // register-blocked dense launch;
     // then heavy jobs (cost at least half the slice target), so that the longest tiles are
     // dispatched first and the light ones fill in behind them.
     int64_t tot3d = 0, tot3h = 0, tot3l = 0;
@@ -596,7 +597,9 @@ __device__ __forceinline__ void res_pack(const ResPtrs& p) {
                 DJob* djp = p.djobs + j;
                 if (djp->cls == 0) {
                     const float cost = l3_cost(jd, *djp);
-                    const bool dense = djp->kind == kJobFam && 16 * (int64_t)p.fams[djp->fam].sup >= p.n_bits;
+                    // a family job, or the lookahead of a family (its head-union-tail mask is a subset
+                    // of the family's prefix, and on a dense family almost never zero per 128 bits)
+                    const bool dense = 16 * (int64_t)p.fams[djp->fam].sup >= p.n_bits;
                     int64_t sl = lmin(max_sl, lmax(1, (int64_t)ceilf(cost / (dense ? target_d : target))));
                     const int64_t wsl = ((W / 64 + sl - 1) / sl) * 64;
                     sl = wsl > 0 ? (W + wsl - 1) / wsl : 1;
