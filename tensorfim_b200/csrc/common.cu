@@ -162,7 +162,7 @@ void tuning_builtin(tfim_tuning* t) {
     t->tc_min_work = 1536;
     t->tc_min_density = 0.5f;
     t->tc_tiles_per_sm = 8.f;
-    t->gram_min_rows = 16;
+    t->gram_min_rows = 32;
     t->l3_dense_slices_per_sm = 128.f;
 }
 
