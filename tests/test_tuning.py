@@ -80,3 +80,22 @@ def test_shipped_table_loads(restore):
         assert t[k] == doc[k]
     for k in ("l3_slices_per_sm", "b1_tiles_per_sm", "rate_b1_bitops", "rate_lop3_bitops", "rate_pair_incr"):
         assert t[k] == pytest.approx(doc[k], rel=1e-6)
+
+
+def test_dense_slices_field(restore, tmp_path):
+    """The dense families' word-slice target is a field of the table like the others: set,
+    range-checked, loaded from a file, and shipped in the committed table."""
+    assert restore["l3_dense_slices_per_sm"] > 0
+    engine.set_tuning(l3_dense_slices_per_sm=48.0)
+    assert engine.tuning()["l3_dense_slices_per_sm"] == 48.0
+    for bad in (0.0, -1.0, 2048.0):
+        with pytest.raises(TfimError):
+            engine.set_tuning(l3_dense_slices_per_sm=bad)
+    assert engine.tuning()["l3_dense_slices_per_sm"] == 48.0
+    p = tmp_path / "t.json"
+    p.write_text(json.dumps({"l3_dense_slices_per_sm": 96.0}))
+    engine.load_tuning(str(p))
+    assert engine.tuning()["l3_dense_slices_per_sm"] == 96.0
+    with open(SHIPPED) as f:
+        shipped = json.load(f)
+    assert shipped["l3_dense_slices_per_sm"] > 0 and shipped["gram_min_rows"] >= 1
