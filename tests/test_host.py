@@ -254,3 +254,80 @@ def test_oracle_parse_matches_read_fimi_on_random_bytes(oracle_mod, tmp_path):
         b_off, b_items = tf.read_fimi(path)
         assert a_off.tolist() == b_off.tolist(), path
         assert a_items.tolist() == b_items.tolist(), path
+
+
+def test_dense_lop3_pair_blocks_cover_each_pair_once():
+    """The dense-family tile of csrc/count_lop3.cu (lop3_dense_impl), restated: for every tile
+    shape the pack emits (1-8 rows x 1-64 columns) and the row block chosen by its row count,
+    the pair blocks of a 256-thread block cover every (row, column) pair of the tile exactly
+    once, every thread index maps to at most one block, at least 8 threads share a block, and
+    every shared-memory sum index stays inside the 8 x 64 accumulator."""
+    threads = 256
+    br_of = {1: 1, 2: 2, 3: 3, 4: 4, 5: 3, 6: 3, 7: 4, 8: 4}
+    bc_of = {1: 16, 2: 8, 3: 5, 4: 4}
+    for nr in range(1, 9):
+        BR = br_of[nr]
+        BC = bc_of[BR]
+        for nc in range(1, 65):
+            rb, cb = -(-nr // BR), -(-nc // BC)
+            nb = rb * cb
+            assert nb <= 32
+            G = threads // nb
+            assert G >= 8
+            seen = {}
+            for tid in range(threads):
+                b = tid // G
+                if b >= nb:
+                    continue
+                br, bc = (b // cb) * BR, (b % cb) * BC
+                for x in range(BR):
+                    for y in range(BC):
+                        r, c = br + x, bc + y
+                        # loads are clamped to the last row / column; only in-tile pairs are summed
+                        assert min(r, nr - 1) < nr and min(c, nc - 1) < nc
+                        if r < nr and c < nc:
+                            assert r * 64 + c < 8 * 64
+                            seen.setdefault((r, c), set()).add(b)
+            assert len(seen) == nr * nc, (nr, nc)
+            assert all(len(v) == 1 for v in seen.values()), (nr, nc)
+
+
+def test_pack_tile_groups_map_back_to_their_jobs():
+    """The resident pack's CUDA-core tile order (csrc/resident.cu res_pack), restated: dense,
+    heavy and light jobs get exclusive prefix sums of their tile counts within their own group
+    (jobs of other groups add zero), tiles are numbered [dense | heavy | light], and the binary
+    search for the last job whose prefix is <= the tile's index within its group
+    (find_job_by_tile) returns the job that owns the tile, with every tile of every job found
+    exactly once."""
+    rng = np.random.Generator(np.random.PCG64(3))
+    for _ in range(200):
+        nj = int(rng.integers(1, 40))
+        grp = rng.integers(0, 3, size=nj)            # 0 dense, 1 heavy, 2 light
+        ntiles = rng.integers(0, 6, size=nj)
+        pref = np.zeros((3, nj), np.int64)
+        tot = [0, 0, 0]
+        for j in range(nj):
+            for g in range(3):
+                pref[g, j] = tot[g]
+            tot[grp[j]] += int(ntiles[j])
+
+        def find(g, t):
+            lo, hi = 0, nj - 1
+            while lo < hi:
+                mid = (lo + hi + 1) >> 1
+                if pref[g, mid] <= t:
+                    lo = mid
+                else:
+                    hi = mid - 1
+            return lo
+
+        owned = {}
+        starts = [0, tot[0], tot[0] + tot[1]]
+        for t in range(sum(tot)):
+            g = 0 if t < starts[1] else 1 if t < starts[2] else 2
+            j = find(g, t - starts[g])
+            local = t - starts[g] - pref[g, j]
+            assert grp[j] == g and 0 <= local < ntiles[j]
+            owned.setdefault(j, []).append(local)
+        for j in range(nj):
+            assert sorted(owned.get(j, [])) == list(range(int(ntiles[j])))
