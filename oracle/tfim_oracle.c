@@ -266,8 +266,13 @@ static void push_mfi(mfi_list* L, const int32_t* items, int32_t n, int32_t freq)
  * the counts of the node at depth k.  The per-node counting is getResFrequency
  * (kernel_bitmap.cu:390-408) with the prefix AND carried from the parent, which gives
  * the same AND. */
+/* A time-bounded sample (tfo_mine_sample) stops descending once this CLOCK_MONOTONIC time
+ * has passed; 0 means no bound.  Set only outside parallel regions. */
+static double g_deadline = 0.0;
+
 static void dfs(const tfo_db* db, int32_t* X, int32_t k, int32_t freqX, uint64_t* masks,
                 int32_t* resAll, mfi_list* L) {
+    if (g_deadline > 0.0 && now_s() > g_deadline) return;
     const int64_t W = db->W64;
     const int32_t d = db->freqItemsNum;
     const double thr = db->frequencyThreshold;
@@ -360,6 +365,7 @@ TFO_API int64_t tfo_mine_sample(tfo_db* db, double budget_s, int nthreads, doubl
     const int32_t d = db->freqItemsNum;
     const int32_t maxDepth = d + 2;
     int64_t nodes = 0;
+    g_deadline = t0 + budget_s;   /* a long root subtree stops at the budget too */
 #ifdef _OPENMP
     if (nthreads <= 0) nthreads = omp_get_max_threads();
 #else
@@ -383,6 +389,7 @@ TFO_API int64_t tfo_mine_sample(tfo_db* db, double budget_s, int nthreads, doubl
         for (int64_t i = 0; i < L.n; i++) free(L.v[i].items);
         free(L.v); free(masks); free(res); free(X);
     }
+    g_deadline = 0.0;
     if (secs) *secs = now_s() - t0;
     return nodes;
 }
