@@ -331,3 +331,38 @@ def test_pack_tile_groups_map_back_to_their_jobs():
             owned.setdefault(j, []).append(local)
         for j in range(nj):
             assert sorted(owned.get(j, [])) == list(range(int(ntiles[j])))
+
+
+def test_header_is_plain_c_and_links(tmp_path):
+    """include/tfim.h compiles as C99 and a C program links against libtfim.so and calls the
+    entry points that need no GPU (version, tuning table, argument checks), as a cgo / FFI
+    binding of the reference's side would."""
+    import shutil
+    if not shutil.which("gcc"):
+        pytest.skip("gcc not available")
+    src = tmp_path / "abi.c"
+    src.write_text(r'''
+#include <stdio.h>
+#include <string.h>
+#include "tfim.h"
+int main(void) {
+    tfim_tuning t;
+    tfim_tuning_get(&t);
+    if (t.wave_rows < 16 || t.l3_dense_slices_per_sm <= 0.f) return 2;
+    tfim_ctx* ctx = 0;
+    const int64_t off[2] = {0, 2};
+    const int32_t items[2] = {1, 2};
+    if (tfim_open_db(off, items, 1, 1.5, 0, &ctx) != TFIM_E_INVALID || ctx) return 3;
+    int64_t rows = 0, n = 0;
+    if (tfim_parse_text(0, -1, 0, 0, 0, 0, 0, &rows, &n) != TFIM_E_INVALID) return 4;
+    printf("%s\n", tfim_version());
+    return 0;
+}
+''')
+    exe = tmp_path / "abi"
+    lib_dir = os.path.dirname(_lib.LIB_PATH)
+    r = subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe),
+                        "-L", lib_dir, "-ltfim", "-Wl,-rpath," + lib_dir], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0 and "sm_100a" in r.stdout, (r.returncode, r.stdout, r.stderr)
