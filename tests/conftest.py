@@ -30,6 +30,15 @@ def load_golden(name):
     return fx
 
 
+def load_golden_full(name):
+    """A full-size fixture of tests/golden/full (the reference's output on a full-size
+    benchmark database)."""
+    with gzip.open(os.path.join(GOLDEN, "full", name + ".json.gz"), "rt") as f:
+        fx = json.load(f)
+    fx["expected"] = {frozenset(s): f for s, f in fx["mfis"]}
+    return fx
+
+
 def golden_input(fx, tmpdir):
     """Path of the fixture's transaction file (synthetic ones are regenerated from their seed)."""
     spec = fx["spec"]

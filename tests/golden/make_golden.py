@@ -14,7 +14,8 @@ Each fixture <name>.json.gz holds the spec, the reference's header statistics an
 as [sorted item list, frequency] pairs.
 
 Run from the repository root:  python tests/golden/make_golden.py [name ...]
-(with names, only those fixtures are regenerated).
+(with names, only those fixtures are regenerated; the full-size fixtures of full/, minutes of
+CPU each, only when named: python tests/golden/make_golden.py cfg5_full cfg4_full).
 """
 from __future__ import annotations
 
@@ -45,6 +46,15 @@ SYNTH = [
     # minimum support lowered from 85% to 6% (at 85% no item is frequent); supports of the
     # 256-replica database are exactly 256x these
     ("cfg3_base_t06", 3, {"replicas": 1}, 0.06),
+]
+
+
+# Full-size databases of the benchmark shapes, stored under full/ (the per-variant fixture
+# tests do not scan it): the reference's multithreaded CPU engine (the same kernel_bitmap.cu,
+# RUN_MODE 2 with every node on its CPU counter, oracle/_ref/tfim_ref_mt) on all host threads.
+FULL = [
+    ("cfg5_full", 5, {}, 0.70),
+    ("cfg4_full", 4, {}, 0.0005),
 ]
 
 
@@ -106,6 +116,17 @@ def main(only: list[str]) -> None:
             mfis, hdr = oracle.run_reference(path, minsup, timeout=1800)
             spec = {"kind": "synth", "config": cfg, "kwargs": kw, "minsup": minsup}
             _dump(name, spec, hdr, mfis)
+        for name, cfg, kw, minsup in FULL:
+            if name not in only:   # minutes each: only when named
+                continue
+            db = synth.generate(cfg, **kw)
+            path = os.path.join(d, name + ".txt")
+            synth.write_fimi(path, db)
+            mfis, hdr = oracle.run_reference(path, minsup, binary=oracle.REF_MT, threads=os.cpu_count() or 1,
+                                             timeout=7200)
+            spec = {"kind": "synth", "config": cfg, "kwargs": kw, "minsup": minsup}
+            _dump(name, spec, hdr, mfis, sub="full", generator="reference engine (kernel_bitmap.cu, RUN_MODE 2, "
+                  "multithreaded CPU counter) built by oracle/Makefile")
         for name, (blob, minsup) in edge_files().items():
             if only and name not in only:
                 continue
@@ -117,17 +138,19 @@ def main(only: list[str]) -> None:
             _dump(name, spec, hdr, mfis)
 
 
-def _dump(name, spec, hdr, mfis):
+def _dump(name, spec, hdr, mfis, sub: str = "",
+          generator: str = "reference engine (kernel_bitmap.cu, RUN_MODE 0) built by oracle/Makefile"):
     keep = ["transNum", "dimension", "itemIDmin", "itemIDmax", "transLengthMin", "transLengthMax", "transLengthMean",
             "dimensionReduced", "transNumReduced", "transLengthReducedMin", "transLengthReducedMax",
             "transLengthReducedMean", "MFIsNumber"]
     out = {
         "spec": spec,
-        "generator": "reference engine (kernel_bitmap.cu, RUN_MODE 0) built by oracle/Makefile",
+        "generator": generator,
         "header": {k: hdr.get(k) for k in keep},
         "mfis": sorted([sorted(s), f] for s, f in mfis.items()),
     }
-    with gzip.open(os.path.join(HERE, name + ".json.gz"), "wt") as f:
+    os.makedirs(os.path.join(HERE, sub), exist_ok=True)
+    with gzip.open(os.path.join(HERE, sub, name + ".json.gz"), "wt") as f:
         json.dump(out, f, separators=(",", ":"))
     print(f"{name}: {len(mfis)} MFIs")
 

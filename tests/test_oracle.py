@@ -71,3 +71,16 @@ def test_oracle_count_wave_kat(oracle_mod):
         exp = np.array([int(np.unpackbits((m & rows[e]).view(np.uint8)).sum()) for e in range(33)])
         assert (counts[i] == exp).all()
         assert nfreq[i] == (exp >= 300).sum()
+
+
+def test_oracle_matches_reference_at_full_size_cfg5(oracle_mod, tmp_path):
+    """The oracle against the reference's own output on configuration 5 at full size
+    (2,000,000 transactions x 60 groups, minsup 70%): tests/golden/full/cfg5_full, produced by
+    the reference's multithreaded CPU engine (make_golden.py)."""
+    from conftest import load_golden_full
+    fx = load_golden_full("cfg5_full")
+    path = golden_input(fx, tmp_path)
+    db = oracle_mod.OracleDB(path, fx["spec"]["minsup"])
+    assert db.mine() == fx["expected"]
+    assert db.info()["trans_num"] == int(fx["header"]["transNum"])
+    db.close()
