@@ -194,6 +194,12 @@ def test_path_rooflines_arithmetic():
     assert abs(p["lop3"]["share_of_counting"] - 2 / 3) < 1e-12
     r = measure.headline_roofline(p, 6000.0, 1e15, "measured", "measured")
     assert r["kernel"] == "k_count_lop3" and r["bound"] == "hbm" and abs(r["frac"] - 1 / 3) < 1e-12
+    assert r["traffic"] is None
+    # a measured DRAM-per-algorithmic-byte ratio scales with each run's algorithmic bytes
+    p = measure.path_rooflines([st, st], hbm_gbs=6000.0, i8_macs=1e15, traffic={"lop3": 0.25})
+    assert p["lop3"]["traffic_per_launch"] == 0.25 * 8e9 / 4 and "traffic_per_launch" not in p["tc"]
+    r = measure.headline_roofline(p, 6000.0, 1e15, "measured", "measured")
+    assert r["traffic"] == 0.5e9
 
 
 def test_family_counter_shared_memory_windows():
